@@ -1,0 +1,134 @@
+/*
+ * paralanczos.h -- C ABI of the B200 (sm_100a) subset-eigenvalue library
+ * libparalanczos_b200.so.
+ *
+ * Computes, for many index sets S of one symmetric matrix A, the eigenvalues
+ * of the principal submatrix A[S,S] by a k-step Lanczos (start vector
+ * all-ones/sqrt(k), FP32 vectors, FP64 alpha/beta, full reorthogonalisation)
+ * and FP64 Sturm bisection of the tridiagonal, plus the restricted-isometry
+ * constant delta_k = max(1 - lambda_min, lambda_max - 1).
+ *
+ * Every function returns a PL_* status (0 = success).  Device-pointer
+ * functions are asynchronous on `stream` (a cudaStream_t passed as void*,
+ * NULL = legacy default stream); host-pointer functions are synchronous.
+ * Plain pointers and sizes only: no C++ or framework types cross this ABI.
+ *
+ * Reference interfaces replaced (ParaLanczos v0.21, file:line in that project):
+ *   pl_solve / pl_solve_host       POS_SYM_SUBMATRIX_KER2 launched by
+ *                                  calculate_subeigs3 (ParaLanczos.cu:1157-1480,
+ *                                  1811-1863) and POS_SYM_SUBMATRIX_KER
+ *                                  (ParaLanczos.cu:857-1154) as MATLAB launches
+ *                                  them (Matlab/gpu_multi_subsvd*.m)
+ *   pl_calculate_subeigs3          calculate_subeigs3, ParaLanczos.h:47,
+ *                                  ParaLanczos.cu:1811-1863
+ *   pl_calculate_subeigs           calculate_subeigs, ParaLanczos.h:43,
+ *                                  ParaLanczos.cu:1725-1765
+ *   pl_calculate_subeigs2          calculate_subeigs2, ParaLanczos.h:45,
+ *                                  ParaLanczos.cu:1768-1808
+ *   pl_calculate_eigs              calculate_eigs, ParaLanczos.h:41,
+ *                                  ParaLanczos.cu:1685-1722
+ *   pl_gen_sets / pl_gen_stream_host  no counterpart: the reference's callers
+ *                                  build subIndex themselves (example2.cu:42-48)
+ * The C++ (name-mangled) drop-in symbols of ParaLanczos.h are declared in
+ * include/ParaLanczos.h and exported by the same library.
+ */
+#ifndef PARALANCZOS_B200_H
+#define PARALANCZOS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define PL_OK 0
+#define PL_EINVAL 1     /* bad argument (pointer, size, k)                    */
+#define PL_ECUDA 2      /* a CUDA runtime call failed (pl_last_cuda_error)     */
+#define PL_ENOMEM 3     /* device or pinned allocation failed                 */
+#define PL_ENOTSUP 4    /* configuration not supported (e.g. k > PL_KMAX)     */
+#define PL_ETIMEDOUT 5  /* a bounded device-side wait gave up                  */
+#define PL_EBUSY 6      /* resource in use (serving queue full)               */
+
+/* ---- per-set status bits (err[] output; the reference's Eigerror) ------- */
+#define PL_SET_OK 0
+#define PL_SET_BREAKDOWN 1  /* Lanczos restarted after an invariant subspace */
+#define PL_SET_NONFINITE 2  /* NaN/Inf in the submatrix or the recurrence    */
+#define PL_SET_BAD_INDEX 4  /* an index outside [0, n)                       */
+#define PL_SET_BAD_K 8      /* k outside [1, PL_KMAX]                         */
+
+/* ---- forms -------------------------------------------------------------- */
+#define PL_FORM_BATCHED 0   /* persistent, binned by k, register-resident    */
+#define PL_FORM_PLAIN 1     /* one set per thread block (k <= 128)           */
+
+#define PL_KMAX 512         /* largest supported subset size                  */
+
+int pl_version(void);                      /* 100*major + minor               */
+const char *pl_status_string(int status);
+int pl_last_cuda_error(void);              /* cudaError_t of the last PL_ECUDA */
+
+/*
+ * Solve every set (device pointers).
+ *   A       n x n symmetric FP32 matrix, row-major, leading dimension lda >= n
+ *   idx     concatenated 0-based index sets
+ *   offsets NULL: uniform k, set s = idx[s*k .. s*k+k-1];
+ *           else CSR (nsets+1 entries), set s = idx[offsets[s] .. offsets[s+1])
+ *   form    PL_FORM_BATCHED or PL_FORM_PLAIN
+ *   lmin, lmax, delta (FP64, nsets), err (int32, nsets): each nullable
+ *   eig     nullable; all k eigenvalues ascending at the set's index offset
+ *   det     nullable; product of the eigenvalues (FP64, nsets)
+ * Per-set problems are reported in err[], not as a failed call.
+ */
+int pl_solve(const float *A, int n, long long lda, const int *idx, const long long *offsets,
+             long long nsets, int k, int form, double *lmin, double *lmax, double *delta,
+             int *err, double *eig, double *det, void *stream);
+
+/* Same with HOST buffers: copies A and the sets in, solves, copies results out
+ * (synchronous).  offsets/eig/det/lmin/lmax/delta/err nullable as above.     */
+int pl_solve_host(const float *A, int n, long long lda, const int *idx, const long long *offsets,
+                  long long nsets, int k, int form, double *lmin, double *lmax, double *delta,
+                  int *err, double *eig, double *det);
+
+/* Device-side uniform-k index sets from the counter-based generator:
+ * idx[s*k ..] = set (first + s) of stream `seed`, k distinct values in [0,n). */
+int pl_gen_sets(unsigned long long seed, long long first, long long nsets, int n, int k, int *idx,
+                void *stream);
+
+/* Host generator of a CSR stream.  kdist: 0 fixed kmin; 1 {8,..,256} with P~1/k;
+ * 2 uniform in [kmin,kmax].  With offsets == idx == NULL it only returns the
+ * total index count.                                                         */
+long long pl_gen_stream_host(unsigned long long seed, long long first, long long nsets, int n,
+                             int kdist, int kmin, int kmax, long long *offsets, int *idx);
+
+/* FP64 -> FP32 conversion on the device (for FP64 matrices). */
+int pl_convert_f64_f32(const double *in, float *out, long long count, void *stream);
+
+/* ---- ParaLanczos.h drop-ins with a status return ------------------------ */
+/* Host pointers, FP64 matrix, all eigenvalues out; semantics of the named
+ * reference routine (validation messages, output layout).  PL_STRICT=0 in the
+ * environment lifts the reference's k <= 128 / k % 4 == 0 limits.           */
+int pl_calculate_subeigs3(double *mat, int subIndexLen, int matsize, double *Eigenvalues,
+                          double *Det, int *subIndex, int subn);
+int pl_calculate_subeigs(double *mat, int n, double *Eigenvalues, double *Det, int *subIndex,
+                         int subn);
+int pl_calculate_subeigs2(double *mat, int n, int matsize, double *Eigenvalues, double *Det,
+                          int *subIndex, int subn);
+int pl_calculate_eigs(double *mat, int n, double *Eigenvalues, double *Det);
+
+/* ---- tuning and measurement --------------------------------------------- */
+/* Select variant `variant` of the kernel shape for bin `bin` (see
+ * pl_tune_describe); -1 restores the default.                                */
+int pl_tune_set(int bin, int variant);
+/* Writes a description of bin/variant into buf (NUL-terminated); returns the
+ * number of variants of `bin`, or 0 for an unknown bin.                      */
+int pl_tune_describe(int bin, int variant, char *buf, int buflen);
+int pl_num_bins(void);
+/* Upper k of bin b. */
+int pl_bin_kmax(int bin);
+/* Measured FP32 FMA throughput of this GPU (TFLOP/s), for roofline figures. */
+int pl_fp32_peak(double *tflops, void *stream);
+/* Releases cached device scratch, graphs and streams of this library. */
+int pl_release(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PARALANCZOS_B200_H */

@@ -1,0 +1,541 @@
+// pl_api.cu -- host dispatch and the C ABI of libparalanczos_b200.so.
+//
+// Replaces the host API of the reference (ParaLanczos.cu:1642-1863, declared in
+// ParaLanczos.h:39-47).  Differences: no cudaDeviceReset, device scratch is
+// cached per device, results and per-set status are returned, nothing is
+// printed unless PL_VERBOSE=1 (then the reference's stdout lines are
+// reproduced), and uneven k is binned on the device and run from a captured
+// CUDA graph.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/paralanczos.h"
+#include "pl_kernels.cuh"
+
+using namespace pl;
+
+namespace {
+
+thread_local int g_last_cuda = 0;
+std::mutex g_mu;
+
+#define PL_CU(call)                              \
+  do {                                           \
+    cudaError_t e_ = (call);                     \
+    if (e_ != cudaSuccess) {                     \
+      g_last_cuda = (int)e_;                     \
+      return e_ == cudaErrorMemoryAllocation ? PL_ENOMEM : PL_ECUDA; \
+    }                                            \
+  } while (0)
+
+int device_sms() {
+  static int sms[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return 148;
+  if (!sms[dev]) cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+  return sms[dev] > 0 ? sms[dev] : 148;
+}
+
+typedef cudaError_t (*LaunchFn)(const MatrixF32&, const SetSource&, const SetOutputs&, long long,
+                                float*, cudaStream_t);
+
+template <class K>
+int occupancy(K kern, int cta, size_t dsmem) {
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, cta, dsmem);
+  return occ > 0 ? occ : 1;
+}
+
+long long grid_for(long long nitems, int per_cta, int occ) {
+  const long long full = (long long)device_sms() * occ;
+  if (nitems < 0) return full;  // count lives on the device
+  const long long need = (nitems + per_cta - 1) / per_cta;
+  return need < full ? (need > 0 ? need : 1) : full;
+}
+
+template <int KB, int RPT, int TPR, int CTA, int MINB, bool ALL>
+cudaError_t launch_reg(const MatrixF32& M, const SetSource& src, const SetOutputs& out,
+                       long long nitems, float*, cudaStream_t st) {
+  auto kern = k_reg_solve<KB, RPT, TPR, CTA, MINB, ALL>;
+  static int occ = occupancy(kern, CTA, 0);
+  constexpr int GPC = CTA / Cfg<KB, RPT, TPR>::NT;
+  const long long grid = grid_for(nitems, GPC, occ);
+  kern<<<(unsigned)grid, CTA, 0, st>>>(M, src, out);
+  return cudaGetLastError();
+}
+
+template <int KB, bool ALL>
+cudaError_t launch_plain(const MatrixF32& M, const SetSource& src, const SetOutputs& out,
+                         long long nitems, float*, cudaStream_t st) {
+  constexpr int NT = KB < 32 ? 32 : KB;
+  const size_t dsm = sizeof(float) * 2 * KB * (KB + 1);
+  auto kern = k_plain<KB, ALL>;
+  static bool attr = [&] {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
+    return true;
+  }();
+  (void)attr;
+  // one set per thread block; grid-stride only beyond the grid limit
+  long long grid = nitems < 0 ? (long long)device_sms() * 16 : nitems;
+  if (grid > 0x7fffffffLL) grid = 0x7fffffffLL;
+  if (grid < 1) grid = 1;
+  kern<<<(unsigned)grid, NT, dsm, st>>>(M, src, out);
+  return cudaGetLastError();
+}
+
+template <int KM, bool ALL>
+cudaError_t launch_large(const MatrixF32& M, const SetSource& src, const SetOutputs& out,
+                         long long nitems, float* scratch, cudaStream_t st) {
+  auto kern = k_large<KM, ALL>;
+  const long long grid = grid_for(nitems, 1, 1);
+  kern<<<(unsigned)grid, 256, 0, st>>>(M, src, out, scratch);
+  return cudaGetLastError();
+}
+
+struct Variant {
+  const char* desc;
+  LaunchFn fn[2];  // [extremes only, all eigenvalues]
+  bool large;      // needs the scratch slots
+  int km;          // scratch k capacity (large only)
+};
+
+#define REG(KB, RPT, TPR, CTA, MINB)                                                          \
+  Variant {                                                                                    \
+    "reg KB=" #KB " RPT=" #RPT " TPR=" #TPR " CTA=" #CTA " MINB=" #MINB,                       \
+        {launch_reg<KB, RPT, TPR, CTA, MINB, false>, launch_reg<KB, RPT, TPR, CTA, MINB, true>}, \
+        false, 0                                                                               \
+  }
+#define LARGE(KM) \
+  Variant { "large KM=" #KM " CTA=256", {launch_large<KM, false>, launch_large<KM, true>}, true, KM }
+
+const int kBinK[] = {8, 16, 32, 64, 128, 256, 512};
+constexpr int kNumBins = 7;
+
+const std::vector<Variant>& variants(int b) {
+  static const std::vector<Variant> v[kNumBins] = {
+      {REG(8, 1, 1, 128, 4), REG(8, 2, 1, 128, 4), REG(8, 1, 1, 256, 4)},
+      {REG(16, 1, 1, 128, 4), REG(16, 2, 1, 128, 4), REG(16, 1, 1, 256, 3)},
+      {REG(32, 1, 1, 128, 4), REG(32, 2, 1, 128, 3), REG(32, 1, 2, 128, 4)},
+      {REG(64, 1, 1, 128, 3), REG(64, 1, 2, 128, 3), REG(64, 1, 1, 64, 6), REG(64, 1, 1, 256, 1)},
+      {REG(128, 1, 2, 256, 1)},
+      {LARGE(256)},
+      {LARGE(512)},
+  };
+  return v[b];
+}
+
+int g_variant[kNumBins] = {0, 0, 0, 0, 0, 0, 0};
+
+int bin_of_k(int k) {
+  for (int b = 0; b < kNumBins; ++b)
+    if (k <= kBinK[b]) return b;
+  return -1;
+}
+
+const Variant& chosen(int b) {
+  const auto& v = variants(b);
+  int i = g_variant[b];
+  if (i < 0 || i >= (int)v.size()) i = 0;
+  return v[i];
+}
+
+// Plain form kernels by k bin (k <= 128).
+LaunchFn plain_fn(int k, bool all) {
+  if (k <= 16) return all ? launch_plain<16, true> : launch_plain<16, false>;
+  if (k <= 32) return all ? launch_plain<32, true> : launch_plain<32, false>;
+  if (k <= 64) return all ? launch_plain<64, true> : launch_plain<64, false>;
+  if (k <= 128) return all ? launch_plain<128, true> : launch_plain<128, false>;
+  return nullptr;
+}
+
+// ----------------------------------------------------------------------------
+// Per-device cached scratch (grow-only).
+// ----------------------------------------------------------------------------
+struct DevScratch {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+struct DevState {
+  DevScratch large;    // k_large slots
+  DevScratch bins;     // counts / starts / cursor / perm
+  DevScratch upload;   // pl_solve_host and drop-in staging
+  cudaStream_t side[kNumBins] = {};
+  cudaEvent_t ev_fork = nullptr;
+  cudaEvent_t ev_join[kNumBins] = {};
+  struct GraphEntry {
+    cudaGraphExec_t exec;
+  };
+  std::unordered_map<std::string, GraphEntry> graphs;
+};
+
+DevState g_state[64];
+
+DevState& state() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  return g_state[dev < 0 || dev >= 64 ? 0 : dev];
+}
+
+void drop_graphs(DevState& d) {
+  for (auto& kv : d.graphs) cudaGraphExecDestroy(kv.second.exec);
+  d.graphs.clear();
+}
+
+// Grow-only scratch.  A reallocation invalidates every cached graph of the
+// device (they hold pointers into the scratch buffers).
+int ensure(DevScratch& s, size_t bytes) {
+  if (s.bytes >= bytes) return PL_OK;
+  DevState& d = state();
+  if (s.p) {
+    cudaDeviceSynchronize();
+    drop_graphs(d);
+    cudaFree(s.p);
+    s.p = nullptr;
+    s.bytes = 0;
+  }
+  PL_CU(cudaMalloc(&s.p, bytes));
+  s.bytes = bytes;
+  return PL_OK;
+}
+
+int ensure_streams(DevState& d) {
+  if (d.ev_fork) return PL_OK;
+  PL_CU(cudaEventCreateWithFlags(&d.ev_fork, cudaEventDisableTiming));
+  for (int b = 0; b < kNumBins; ++b) {
+    PL_CU(cudaStreamCreateWithFlags(&d.side[b], cudaStreamNonBlocking));
+    PL_CU(cudaEventCreateWithFlags(&d.ev_join[b], cudaEventDisableTiming));
+  }
+  return PL_OK;
+}
+
+bool env_flag(const char* name, bool dflt) {
+  const char* v = getenv(name);
+  if (!v || !*v) return dflt;
+  return !(v[0] == '0' || v[0] == 'n' || v[0] == 'N' || v[0] == 'f' || v[0] == 'F');
+}
+
+// Uniform k: one kernel.
+int solve_uniform(const MatrixF32& M, const int* idx, long long nsets, int k, int form,
+                  const SetOutputs& out, cudaStream_t st) {
+  const bool all = out.eig || out.det;
+  SetSource src{idx, nullptr, k, nullptr, nullptr, nullptr, nsets};
+  if (form == PL_FORM_PLAIN && k <= 128) {
+    PL_CU(plain_fn(k, all)(M, src, out, nsets, nullptr, st));
+    return PL_OK;
+  }
+  const int b = bin_of_k(k);
+  if (b < 0) return PL_ENOTSUP;
+  const Variant& v = chosen(b);
+  float* scratch = nullptr;
+  if (v.large) {
+    const long long slots = grid_for(nsets, 1, 1);
+    int rc = ensure(state().large, sizeof(float) * 2 * (size_t)v.km * v.km * (size_t)slots);
+    if (rc) return rc;
+    scratch = (float*)state().large.p;
+  }
+  PL_CU(v.fn[all ? 1 : 0](M, src, out, nsets, scratch, st));
+  return PL_OK;
+}
+
+// Uneven k (CSR): device binning, then one persistent launch per non-empty
+// bin on forked streams, all captured into one CUDA graph (cached by the call
+// signature) and launched as one unit.
+int solve_csr(const MatrixF32& M, const int* idx, const long long* offsets, long long nsets,
+              int form, const SetOutputs& out, cudaStream_t st) {
+  const bool all = out.eig || out.det;
+  DevState& d = state();
+  int rc = ensure_streams(d);
+  if (rc) return rc;
+  const int nb = kNumBins;
+  const size_t hdr = 3 * 16;  // counts / starts / cursor, 16 ints each
+  rc = ensure(d.bins, sizeof(int) * (hdr + (size_t)nsets));
+  if (rc) return rc;
+  // every large-k bin gets its own scratch region: the bins run concurrently
+  const long long slots = device_sms();
+  size_t large_off[kNumBins] = {0};
+  size_t large_total = 0;
+  for (int b = 0; b < nb; ++b) {
+    large_off[b] = large_total;
+    if (chosen(b).large) large_total += 2 * (size_t)chosen(b).km * chosen(b).km * (size_t)slots;
+  }
+  rc = ensure(d.large, sizeof(float) * (large_total > 0 ? large_total : 1));
+  if (rc) return rc;
+  char keybuf[512];
+  snprintf(keybuf, sizeof keybuf, "%p|%d|%lld|%p|%p|%lld|%d|%p|%p|%p|%p|%p|%p|%p|%d%d%d%d%d%d%d",
+           (const void*)M.A, M.n, M.lda, (const void*)idx, (const void*)offsets, nsets, form,
+           (void*)out.lmin, (void*)out.lmax, (void*)out.delta, (void*)out.err, (void*)out.eig,
+           (void*)out.det, (void*)st, g_variant[0], g_variant[1], g_variant[2], g_variant[3],
+           g_variant[4], g_variant[5], g_variant[6]);
+  const std::string key(keybuf);
+  auto it = d.graphs.find(key);
+  if (it == d.graphs.end()) {
+    int* counts = (int*)d.bins.p;
+    int* starts = counts + 16;
+    int* cursor = counts + 32;
+    int* perm = counts + 48;
+    BinTable bt;
+    bt.nb = nb;
+    for (int b = 0; b < nb; ++b) bt.kmax[b] = kBinK[b];
+    cudaStream_t cs = st;
+    cudaStreamCaptureStatus cst;
+    PL_CU(cudaStreamIsCapturing(cs, &cst));
+    if (cst != cudaStreamCaptureStatusNone) return PL_EINVAL;
+    PL_CU(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    cudaMemsetAsync(counts, 0, sizeof(int) * 16, cs);
+    const int tb = 256;
+    const long long g = (nsets + tb - 1) / tb;
+    const unsigned grid = (unsigned)(g < 4096 ? (g > 0 ? g : 1) : 4096);
+    k_bin_count<<<grid, tb, 0, cs>>>(offsets, nsets, bt, counts);
+    k_bin_scan<<<1, 32, 0, cs>>>(counts, nb, starts, cursor);
+    k_bin_scatter<<<grid, tb, 0, cs>>>(offsets, nsets, bt, starts, cursor, perm);
+    k_mark_bad_k<<<64, 256, 0, cs>>>(perm, starts + nb, counts + nb, offsets, out);
+    cudaEventRecord(d.ev_fork, cs);
+    // largest-k bins first so the small-k kernels fill the tail
+    for (int b = nb - 1; b >= 0; --b) {
+      cudaStreamWaitEvent(d.side[b], d.ev_fork, 0);
+      SetSource src{idx, offsets, 0, perm, starts + b, counts + b, 0};
+      cudaError_t e;
+      if (form == PL_FORM_PLAIN && kBinK[b] <= 128) {
+        e = plain_fn(kBinK[b], all)(M, src, out, -1, nullptr, d.side[b]);
+      } else {
+        const Variant& v = chosen(b);
+        e = v.fn[all ? 1 : 0](M, src, out, -1, (float*)d.large.p + large_off[b], d.side[b]);
+      }
+      if (e != cudaSuccess) {
+        cudaGraph_t gr;
+        cudaStreamEndCapture(cs, &gr);
+        if (gr) cudaGraphDestroy(gr);
+        g_last_cuda = (int)e;
+        return PL_ECUDA;
+      }
+      cudaEventRecord(d.ev_join[b], d.side[b]);
+      cudaStreamWaitEvent(cs, d.ev_join[b], 0);
+    }
+    cudaGraph_t graph = nullptr;
+    PL_CU(cudaStreamEndCapture(cs, &graph));
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    PL_CU(e);
+    it = d.graphs.emplace(key, DevState::GraphEntry{exec}).first;
+  }
+  PL_CU(cudaGraphLaunch(it->second.exec, st));
+  return PL_OK;
+}
+
+int validate_common(const float* A, int n, long long lda, const int* idx, long long nsets, int k,
+                    const long long* offsets, int form) {
+  if (nsets < 0 || n <= 0 || lda < n) return PL_EINVAL;
+  if (nsets == 0) return PL_OK;
+  if (!A || !idx) return PL_EINVAL;
+  if (form != PL_FORM_BATCHED && form != PL_FORM_PLAIN) return PL_EINVAL;
+  if (!offsets) {
+    if (k < 1) return PL_EINVAL;
+    if (k > PL_KMAX) return PL_ENOTSUP;
+    if (k > n) return PL_EINVAL;
+  }
+  return PL_OK;
+}
+
+int solve_dev(const float* A, int n, long long lda, const int* idx, const long long* offsets,
+              long long nsets, int k, int form, const SetOutputs& out, cudaStream_t st) {
+  int rc = validate_common(A, n, lda, idx, nsets, k, offsets, form);
+  if (rc || nsets == 0) return rc;
+  MatrixF32 M{A, lda, n};
+  if (!offsets) return solve_uniform(M, idx, nsets, k, form, out, st);
+  return solve_csr(M, idx, offsets, nsets, form, out, st);
+}
+
+// Staging for host-buffer calls: one grow-only device buffer carved in place.
+struct Carve {
+  char* base;
+  size_t off;
+  template <class T>
+  T* take(size_t count) {
+    off = (off + 255) & ~(size_t)255;
+    T* p = (T*)(base + off);
+    off += sizeof(T) * count;
+    return p;
+  }
+};
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+// =============================================================================
+// C ABI
+// =============================================================================
+extern "C" {
+
+int pl_version(void) { return 100; }
+
+const char* pl_status_string(int s) {
+  switch (s) {
+    case PL_OK: return "ok";
+    case PL_EINVAL: return "invalid argument";
+    case PL_ECUDA: return "CUDA error";
+    case PL_ENOMEM: return "out of memory";
+    case PL_ENOTSUP: return "not supported";
+    case PL_ETIMEDOUT: return "timed out";
+    case PL_EBUSY: return "busy";
+    default: return "unknown status";
+  }
+}
+
+int pl_last_cuda_error(void) { return g_last_cuda; }
+
+int pl_solve(const float* A, int n, long long lda, const int* idx, const long long* offsets,
+             long long nsets, int k, int form, double* lmin, double* lmax, double* delta, int* err,
+             double* eig, double* det, void* stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  SetOutputs out{lmin, lmax, delta, err, eig, det};
+  return solve_dev(A, n, lda, idx, offsets, nsets, k, form, out, (cudaStream_t)stream);
+}
+
+int pl_solve_host(const float* A, int n, long long lda, const int* idx, const long long* offsets,
+                  long long nsets, int k, int form, double* lmin, double* lmax, double* delta,
+                  int* err, double* eig, double* det) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  int rc = validate_common(A, n, lda, idx, nsets, k, offsets, form);
+  if (rc || nsets == 0) return rc;
+  long long total = offsets ? offsets[nsets] : nsets * (long long)k;
+  if (offsets && offsets[0] != 0) return PL_EINVAL;
+  const size_t bytes = align256(sizeof(float) * (size_t)n * lda) + align256(sizeof(int) * total) +
+                       align256(sizeof(long long) * (nsets + 1)) + 4 * align256(sizeof(double) * nsets) +
+                       align256(sizeof(int) * nsets) + align256(sizeof(double) * total) + 4096;
+  DevState& d = state();
+  rc = ensure(d.upload, bytes);
+  if (rc) return rc;
+  Carve cv{(char*)d.upload.p, 0};
+  float* dA = cv.take<float>((size_t)n * lda);
+  int* dI = cv.take<int>(total);
+  long long* dO = offsets ? cv.take<long long>(nsets + 1) : nullptr;
+  double* dmin = lmin ? cv.take<double>(nsets) : nullptr;
+  double* dmax = lmax ? cv.take<double>(nsets) : nullptr;
+  double* ddel = delta ? cv.take<double>(nsets) : nullptr;
+  double* ddet = det ? cv.take<double>(nsets) : nullptr;
+  int* derr = err ? cv.take<int>(nsets) : nullptr;
+  double* deig = eig ? cv.take<double>(total) : nullptr;
+  cudaStream_t st = 0;
+  PL_CU(cudaMemcpyAsync(dA, A, sizeof(float) * (size_t)n * lda, cudaMemcpyHostToDevice, st));
+  PL_CU(cudaMemcpyAsync(dI, idx, sizeof(int) * total, cudaMemcpyHostToDevice, st));
+  if (dO) PL_CU(cudaMemcpyAsync(dO, offsets, sizeof(long long) * (nsets + 1), cudaMemcpyHostToDevice, st));
+  SetOutputs out{dmin, dmax, ddel, derr, deig, ddet};
+  rc = solve_dev(dA, n, lda, dI, dO, nsets, k, form, out, st);
+  if (rc) return rc;
+  if (lmin) PL_CU(cudaMemcpyAsync(lmin, dmin, sizeof(double) * nsets, cudaMemcpyDeviceToHost, st));
+  if (lmax) PL_CU(cudaMemcpyAsync(lmax, dmax, sizeof(double) * nsets, cudaMemcpyDeviceToHost, st));
+  if (delta) PL_CU(cudaMemcpyAsync(delta, ddel, sizeof(double) * nsets, cudaMemcpyDeviceToHost, st));
+  if (det) PL_CU(cudaMemcpyAsync(det, ddet, sizeof(double) * nsets, cudaMemcpyDeviceToHost, st));
+  if (err) PL_CU(cudaMemcpyAsync(err, derr, sizeof(int) * nsets, cudaMemcpyDeviceToHost, st));
+  if (eig) PL_CU(cudaMemcpyAsync(eig, deig, sizeof(double) * total, cudaMemcpyDeviceToHost, st));
+  PL_CU(cudaStreamSynchronize(st));
+  return PL_OK;
+}
+
+int pl_gen_sets(unsigned long long seed, long long first, long long nsets, int n, int k, int* idx,
+                void* stream) {
+  if (nsets < 0 || k < 1 || k > n || (nsets > 0 && !idx)) return PL_EINVAL;
+  if (nsets == 0) return PL_OK;
+  const long long g = (nsets + 255) / 256;
+  k_gen_sets<<<(unsigned)(g < 65535 ? g : 65535), 256, 0, (cudaStream_t)stream>>>(seed, first, nsets,
+                                                                                   n, k, idx);
+  PL_CU(cudaGetLastError());
+  return PL_OK;
+}
+
+long long pl_gen_stream_host(unsigned long long seed, long long first, long long nsets, int n,
+                             int kdist, int kmin, int kmax, long long* offsets, int* idx) {
+  long long off = 0;
+  for (long long s = 0; s < nsets; ++s) {
+    const int k = gen_k(seed, (uint64_t)(first + s), kdist, kmin, kmax);
+    if (offsets) offsets[s] = off;
+    if (idx) gen_set(seed, (uint64_t)(first + s), n, k, idx + off);
+    off += k;
+  }
+  if (offsets) offsets[nsets] = off;
+  return off;
+}
+
+int pl_convert_f64_f32(const double* in, float* out, long long count, void* stream) {
+  if (count < 0 || (count > 0 && (!in || !out))) return PL_EINVAL;
+  if (count == 0) return PL_OK;
+  const long long g = (count + 255) / 256;
+  k_f64_to_f32<<<(unsigned)(g < 8192 ? g : 8192), 256, 0, (cudaStream_t)stream>>>(in, out, count);
+  PL_CU(cudaGetLastError());
+  return PL_OK;
+}
+
+int pl_tune_set(int bin, int variant) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (bin < 0 || bin >= kNumBins) return PL_EINVAL;
+  if (variant >= (int)variants(bin).size()) return PL_EINVAL;
+  g_variant[bin] = variant < 0 ? 0 : variant;
+  return PL_OK;
+}
+
+int pl_tune_describe(int bin, int variant, char* buf, int buflen) {
+  if (bin < 0 || bin >= kNumBins) return 0;
+  const auto& v = variants(bin);
+  if (buf && buflen > 0) {
+    const char* s = (variant >= 0 && variant < (int)v.size()) ? v[variant].desc : "";
+    snprintf(buf, (size_t)buflen, "%s", s);
+  }
+  return (int)v.size();
+}
+
+int pl_num_bins(void) { return kNumBins; }
+
+int pl_bin_kmax(int bin) { return (bin >= 0 && bin < kNumBins) ? kBinK[bin] : 0; }
+
+int pl_fp32_peak(double* tflops, void* stream) {
+  if (!tflops) return PL_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  float* dummy = nullptr;
+  PL_CU(cudaMalloc(&dummy, 256 * sizeof(float)));
+  cudaEvent_t e0, e1;
+  PL_CU(cudaEventCreate(&e0));
+  PL_CU(cudaEventCreate(&e1));
+  const int grid = device_sms() * 8, iters = 2048;
+  k_fma_peak<<<grid, 256, 0, st>>>(dummy, iters, 0.999f);  // warm-up
+  cudaEventRecord(e0, st);
+  k_fma_peak<<<grid, 256, 0, st>>>(dummy, iters, 0.999f);
+  cudaEventRecord(e1, st);
+  PL_CU(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(dummy);
+  const double flops = 2.0 * 8 * 16 * (double)iters * grid * 256;
+  *tflops = flops / (ms * 1e-3) / 1e12;
+  PL_CU(cudaGetLastError());
+  return PL_OK;
+}
+
+int pl_release(void) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  cudaDeviceSynchronize();
+  DevState& d = state();
+  for (auto& kv : d.graphs) cudaGraphExecDestroy(kv.second.exec);
+  d.graphs.clear();
+  for (DevScratch* s : {&d.large, &d.bins, &d.upload}) {
+    if (s->p) cudaFree(s->p);
+    s->p = nullptr;
+    s->bytes = 0;
+  }
+  return PL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,63 @@
+// pl_common.cuh -- shared definitions for the sm_100a subset-eigenvalue kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pl {
+
+// Per-set status bits written to err[] (the reference's Eigerror is TQLRAT's
+// ierr, ParaLanczos.cu:1467; these extend it).
+enum SetStatus : int {
+  SET_OK = 0,
+  SET_BREAKDOWN = 1,     // a Lanczos step had beta below the breakdown threshold;
+                         // the recurrence was restarted (result still valid)
+  SET_NONFINITE = 2,     // NaN/Inf met in the submatrix or the recurrence
+  SET_BAD_INDEX = 4,     // an index of the set is outside [0, n)
+  SET_BAD_K = 8,         // the set's k is outside the kernel's supported range
+};
+
+constexpr float kEps32 = 1.1920929e-7f;
+
+// Where one launch reads its sets from.
+struct SetSource {
+  const int* idx;            // concatenated index sets (0-based rows/cols of A)
+  const long long* offsets;  // CSR offsets (nsets+1) or nullptr for uniform k
+  int k;                     // uniform k (offsets == nullptr)
+  const int* perm;           // optional work-item -> set id map (binned queues)
+  const int* perm_start;     // optional device-side offset of this queue in perm
+  const int* count;          // optional device-side work-item count (binned queues)
+  long long nitems;          // work items when count == nullptr
+};
+
+struct SetOutputs {
+  double* lmin;   // lambda_min per set (nullable)
+  double* lmax;   // lambda_max per set (nullable)
+  double* delta;  // delta_k = max(1 - lambda_min, lambda_max - 1) (nullable)
+  int* err;       // SetStatus bits (nullable)
+  double* eig;    // all k eigenvalues ascending at the set's index offset (nullable)
+  double* det;    // product of eigenvalues (nullable)
+};
+
+struct MatrixF32 {
+  const float* A;  // symmetric, row-major
+  long long lda;
+  int n;
+};
+
+__device__ __forceinline__ long long item_count(const SetSource& src) {
+  return src.count ? (long long)(*src.count) : src.nitems;
+}
+
+__device__ __forceinline__ void set_span(const SetSource& src, long long item, int pbase,
+                                         long long& set, long long& off, int& k) {
+  set = src.perm ? (long long)src.perm[pbase + item] : item;
+  if (src.offsets) {
+    off = src.offsets[set];
+    k = (int)(src.offsets[set + 1] - off);
+  } else {
+    off = set * (long long)src.k;
+    k = src.k;
+  }
+}
+
+}  // namespace pl

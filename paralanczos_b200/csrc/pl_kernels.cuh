@@ -1,0 +1,200 @@
+// pl_kernels.cuh -- __global__ kernels of the library (one translation unit
+// includes this: pl_api.cu).
+#pragma once
+#include "pl_cgs.cuh"
+#include "pl_engine.cuh"
+#include "pl_indexgen.cuh"
+
+namespace pl {
+
+// ---------------------------------------------------------------------------
+// Batched form: persistent, register-resident engine for one k bin.
+// Each group of NT threads takes work items gid, gid + ngroups, ...
+// ---------------------------------------------------------------------------
+template <int KB, int RPT, int TPR, int CTA, int MINB, bool ALL>
+__global__ void __launch_bounds__(CTA, MINB)
+    k_reg_solve(MatrixF32 M, SetSource src, SetOutputs out) {
+  using C = Cfg<KB, RPT, TPR>;
+  constexpr int GPC = CTA / C::NT;
+  static_assert(CTA % C::NT == 0, "CTA must hold whole groups");
+  static_assert(C::NT <= 32 || GPC <= 15, "named barrier ids");
+  __shared__ GroupSmem<KB, C::NW> smem[GPC];
+  const Grp<C::NT> g = make_group<C::NT>();
+  const int gic = threadIdx.x / C::NT;
+  const long long ng = (long long)gridDim.x * GPC;
+  const long long nitems = item_count(src);
+  const int pbase = src.perm_start ? *src.perm_start : 0;
+  for (long long it = (long long)blockIdx.x * GPC + gic; it < nitems; it += ng) {
+    long long set, off;
+    int k;
+    set_span(src, it, pbase, set, off, k);
+    if (k < 1 || k > KB) {
+      if (g.t == 0) write_failed(out, set, off, 0, SET_BAD_K);
+      continue;
+    }
+    solve_set<KB, RPT, TPR, ALL>(M, src.idx + off, k, set, off, out, smem[gic], g);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Plain form: one set per thread block (grid-stride over sets), A_S and V in
+// shared memory.  Dynamic shared memory: 2 * KB * (KB + 1) floats.
+// ---------------------------------------------------------------------------
+template <int KB, bool ALL>
+__global__ void __launch_bounds__(KB < 32 ? 32 : KB)
+    k_plain(MatrixF32 M, SetSource src, SetOutputs out) {
+  constexpr int NT = KB < 32 ? 32 : KB;
+  constexpr int NW = NT / 32;
+  extern __shared__ __align__(16) float dsm[];
+  __shared__ CgsSmem<KB, NW> sm;
+  float* As = dsm;
+  float* V = dsm + KB * (KB + 1);
+  const Grp<NT> g = make_group<NT>();
+  const long long nitems = item_count(src);
+  const int pbase = src.perm_start ? *src.perm_start : 0;
+  for (long long it = blockIdx.x; it < nitems; it += gridDim.x) {
+    long long set, off;
+    int k;
+    set_span(src, it, pbase, set, off, k);
+    if (k < 1 || k > KB) {
+      if (g.t == 0) write_failed(out, set, off, 0, SET_BAD_K);
+      continue;
+    }
+    cgs_solve_set<NT, 1, KB, ALL>(M, src.idx + off, k, set, off, out, As, KB + 1, V, KB + 1, sm, g);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Large-k form (k <= KM): persistent, one set per CTA at a time, A_S and V in
+// the CTA's scratch slot (2 * KM * KM floats, L2-resident when it fits).
+// ---------------------------------------------------------------------------
+template <int KM, bool ALL>
+__global__ void __launch_bounds__(256, 1)
+    k_large(MatrixF32 M, SetSource src, SetOutputs out, float* __restrict__ scratch) {
+  constexpr int NT = 256;
+  constexpr int RM = (KM + NT - 1) / NT;
+  __shared__ CgsSmem<KM, NT / 32> sm;
+  const Grp<NT> g = make_group<NT>();
+  float* As = scratch + (size_t)blockIdx.x * (size_t)(2 * KM * KM);
+  float* V = As + (size_t)KM * KM;
+  const long long nitems = item_count(src);
+  const int pbase = src.perm_start ? *src.perm_start : 0;
+  for (long long it = blockIdx.x; it < nitems; it += gridDim.x) {
+    long long set, off;
+    int k;
+    set_span(src, it, pbase, set, off, k);
+    if (k < 1 || k > KM) {
+      if (g.t == 0) write_failed(out, set, off, 0, SET_BAD_K);
+      continue;
+    }
+    const int ld = (k + 3) & ~3;
+    cgs_solve_set<NT, RM, KM, ALL>(M, src.idx + off, k, set, off, out, As, ld, V, ld, sm, g);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Binning of a CSR set list by k (device-side counting sort of set ids).
+// ---------------------------------------------------------------------------
+constexpr int kMaxBins = 8;
+
+struct BinTable {
+  int nb;
+  int kmax[kMaxBins];  // bin b holds sets with kmax[b-1] < k <= kmax[b]
+};
+
+__device__ __forceinline__ int bin_of(const BinTable& bt, int k) {
+  for (int b = 0; b < bt.nb; ++b)
+    if (k <= bt.kmax[b]) return b;
+  return bt.nb;  // overflow bin (k too large): reported per set
+}
+
+// counts[0..nb] (nb+1 entries, last = overflow) must be zero on entry.
+__global__ void k_bin_count(const long long* __restrict__ offsets, long long nsets, BinTable bt,
+                            int* __restrict__ counts) {
+  __shared__ int h[kMaxBins + 1];
+  if (threadIdx.x <= kMaxBins) h[threadIdx.x] = 0;
+  __syncthreads();
+  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nsets;
+       s += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(offsets[s + 1] - offsets[s]);
+    atomicAdd(&h[bin_of(bt, k)], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x <= bt.nb && h[threadIdx.x]) atomicAdd(&counts[threadIdx.x], h[threadIdx.x]);
+}
+
+// starts[b] = exclusive prefix of counts; cursor[b] = 0.
+__global__ void k_bin_scan(const int* __restrict__ counts, int nb, int* __restrict__ starts,
+                           int* __restrict__ cursor) {
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int b = 0; b <= nb; ++b) {
+      starts[b] = acc;
+      cursor[b] = 0;
+      acc += counts[b];
+    }
+  }
+}
+
+__global__ void k_bin_scatter(const long long* __restrict__ offsets, long long nsets, BinTable bt,
+                              const int* __restrict__ starts, int* __restrict__ cursor,
+                              int* __restrict__ perm) {
+  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nsets;
+       s += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(offsets[s + 1] - offsets[s]);
+    const int b = bin_of(bt, k);
+    const int p = atomicAdd(&cursor[b], 1);
+    perm[starts[b] + p] = (int)s;
+  }
+}
+
+// Sets in the overflow bin get SET_BAD_K.
+__global__ void k_mark_bad_k(const int* __restrict__ perm, const int* __restrict__ start,
+                             const int* __restrict__ count, const long long* __restrict__ offsets,
+                             SetOutputs out) {
+  const int n = *count, base = *start;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const long long s = perm[base + i];
+    write_failed(out, s, offsets[s], 0, SET_BAD_K);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Utilities
+// ---------------------------------------------------------------------------
+__global__ void k_f64_to_f32(const double* __restrict__ in, float* __restrict__ out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+
+// Uniform-k index sets from the counter-based generator: one thread per set.
+__global__ void k_gen_sets(unsigned long long seed, long long first, long long nsets, int n, int k,
+                           int* __restrict__ idx) {
+  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nsets;
+       s += (long long)gridDim.x * blockDim.x)
+    gen_set(seed, (unsigned long long)(first + s), n, k, idx + s * (long long)k);
+}
+
+// FP32 FMA throughput probe (8 independent chains per thread).
+__global__ void __launch_bounds__(256) k_fma_peak(float* out, int iters, float a) {
+  float x0 = threadIdx.x * 1e-3f, x1 = x0 + 1.f, x2 = x0 + 2.f, x3 = x0 + 3.f;
+  float x4 = x0 + 4.f, x5 = x0 + 5.f, x6 = x0 + 6.f, x7 = x0 + 7.f;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      x0 = fmaf(x0, a, 0.5f);
+      x1 = fmaf(x1, a, 0.5f);
+      x2 = fmaf(x2, a, 0.5f);
+      x3 = fmaf(x3, a, 0.5f);
+      x4 = fmaf(x4, a, 0.5f);
+      x5 = fmaf(x5, a, 0.5f);
+      x6 = fmaf(x6, a, 0.5f);
+      x7 = fmaf(x7, a, 0.5f);
+    }
+  }
+  const float s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (s == 12345.678f) out[threadIdx.x] = s;  // keeps the chains live
+}
+
+}  // namespace pl

@@ -1,0 +1,317 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle (the
+reference's per-set algorithm restated in FP64, ParaLanczos.cu:1285-1374 +
+TQLRAT) and FP64 LAPACK dsyev on the same submatrices.
+
+Tolerance (the project's stated bar): every eigenvalue within 1e-5 relative of
+FP64 dsyev on the same (FP32-valued) submatrix; lambda_min / lambda_max within
+1e-5 relative of the oracle.  Index handling is exact: the same subIndex gives
+the same submatrix and the same output slots.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from paralanczos_b200 import _lib, api
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+RTOL = 1e-5
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def gram(M, N, seed, kind="gauss"):
+    rng = np.random.default_rng(seed)
+    if kind == "gauss":
+        Phi = rng.standard_normal((M, N)) / np.sqrt(M)
+    else:
+        Phi = rng.choice([-1.0, 1.0], size=(M, N)) / np.sqrt(M)
+    return (Phi.T @ Phi).astype(np.float32)
+
+
+_CACHE = {}
+
+
+def cached_gram(M, N, seed=0):
+    key = (M, N, seed)
+    if key not in _CACHE:
+        _CACHE[key] = gram(M, N, seed)
+    return _CACHE[key]
+
+
+def dev(x):
+    return _torch().from_numpy(np.ascontiguousarray(x)).cuda()
+
+
+def run(A, idx, k=None, offsets=None, form="batched", want_all=False):
+    torch = _torch()
+    out = api.solve(dev(A), dev(idx), k=k, offsets=None if offsets is None else dev(offsets),
+                    form=form, want_all=want_all)
+    torch.cuda.synchronize()
+    return {n: t.cpu().numpy() for n, t in out.items()}
+
+
+def check_vs_dsyev(A, idx, k, res, offsets=None, all_k=True):
+    truth = O.dsyev_batch(A, idx, k=k, offsets=offsets)
+    for s, t in enumerate(truth):
+        assert abs(res["lmin"][s] - t[0]) <= RTOL * abs(t[0]), (s, res["lmin"][s], t[0])
+        assert abs(res["lmax"][s] - t[-1]) <= RTOL * abs(t[-1]), (s, res["lmax"][s], t[-1])
+        assert res["delta"][s] == max(1 - res["lmin"][s], res["lmax"][s] - 1)
+        if all_k and "eig" in res:
+            lo = offsets[s] if offsets is not None else s * k
+            e = res["eig"][lo:lo + len(t)]
+            np.testing.assert_array_less(np.abs(e - t), RTOL * np.abs(t) + 1e-12)
+            np.testing.assert_allclose(res["det"][s], np.prod(t), rtol=1e-4)
+    return truth
+
+
+@pytest.mark.parametrize("k", [2, 3, 4, 7, 8, 12, 16, 24, 31, 32, 48, 64, 96, 128])
+@pytest.mark.parametrize("form", ["batched", "plain"])
+def test_uniform_k_vs_oracle_and_dsyev(k, form):
+    A = cached_gram(1024, 2048)
+    nsets = 96 if k <= 64 else 24
+    o, idx = O.gen_stream(1, 0, nsets, A.shape[0], 0, k, k)
+    res = run(A, idx, k=k, form=form)
+    assert (res["err"] == 0).all()
+    orc = O.batch(A, idx, k=k)
+    np.testing.assert_array_less(np.abs(res["lmin"] - orc["lmin"]), RTOL * np.abs(orc["lmin"]))
+    np.testing.assert_array_less(np.abs(res["lmax"] - orc["lmax"]), RTOL * np.abs(orc["lmax"]))
+    check_vs_dsyev(A, idx, k, res, all_k=False)
+
+
+@pytest.mark.parametrize("k", [4, 16, 64, 128, 200])
+def test_all_eigenvalues_vs_dsyev(k):
+    A = cached_gram(1024, 2048)
+    nsets = 32 if k <= 64 else 8
+    o, idx = O.gen_stream(2, 0, nsets, A.shape[0], 0, k, k)
+    res = run(A, idx, k=k, want_all=True)
+    assert (res["err"] == 0).all()
+    check_vs_dsyev(A, idx, k, res)
+
+
+@pytest.mark.parametrize("k", [160, 256, 384, 512])
+def test_large_k_vs_dsyev(k):
+    A = cached_gram(2048, 4096) if k > 256 else cached_gram(1024, 2048)
+    nsets = 4
+    o, idx = O.gen_stream(3, 0, nsets, A.shape[0], 0, k, k)
+    res = run(A, idx, k=k)
+    assert (res["err"] == 0).all()
+    check_vs_dsyev(A, idx, k, res, all_k=False)
+
+
+def test_uneven_k_csr_vs_dsyev():
+    A = cached_gram(1024, 4096)
+    offs, idx = O.gen_stream(5, 0, 600, 4096, 1, 8, 256)
+    res = run(A, idx, offsets=offs)
+    assert (res["err"] == 0).all()
+    check_vs_dsyev(A, idx, None, res, offsets=offs, all_k=False)
+    # the captured graph is reused on the second call: same results, bitwise
+    res2 = run(A, idx, offsets=offs)
+    for n in ("lmin", "lmax", "delta", "err"):
+        np.testing.assert_array_equal(res[n], res2[n])
+
+
+def test_uneven_k_plain_form_and_all():
+    A = cached_gram(1024, 2048)
+    offs, idx = O.gen_stream(6, 0, 200, 2048, 2, 2, 140)
+    for form in ("plain", "batched"):
+        res = run(A, idx, offsets=offs, form=form, want_all=True)
+        assert (res["err"] == 0).all()
+        check_vs_dsyev(A, idx, None, res, offsets=offs)
+
+
+def test_golden_submatrices():
+    z = np.load(os.path.join(GOLD, "oracle_sets.npz"))
+    for tag in sorted({k[:-4] for k in z.files if k.endswith("_sub")}):
+        sub = z[tag + "_sub"]
+        nsets, k, _ = sub.shape
+        for s in range(nsets):
+            idx = np.arange(k, dtype=np.int32)
+            res = run(sub[s], idx, k=k, want_all=True)
+            t = z[tag + "_dsyev_eig"][s]
+            np.testing.assert_array_less(np.abs(res["eig"] - t), RTOL * np.abs(t))
+            oe = z[tag + "_oracle_eig"][s]
+            assert abs(res["lmin"][0] - oe[0]) <= RTOL * abs(oe[0])
+            assert abs(res["lmax"][0] - oe[-1]) <= RTOL * abs(oe[-1])
+
+
+# ----------------------------------------------------------------------------- drop-ins
+
+
+def _fixture():
+    fx = json.load(open(os.path.join(GOLD, "fixture8.json")))
+    return np.array(fx["matrix"]).reshape(8, 8), fx
+
+
+def test_dropin_example2_shape():
+    # example2.cu: subset {1,3,5,7} repeated 32 times, subIndexLen 128, minor 4
+    g, fx = _fixture()
+    sub = np.tile(np.array([1, 3, 5, 7], np.int32), 32)
+    eig = np.zeros(128)
+    det = np.zeros(32)
+    assert api.calculate_subeigs3(g.copy(), 128, 8, eig, det, sub, 4) == 0
+    t = np.array(fx["cases"][0]["dsyev_eigs"])
+    for s in range(32):
+        np.testing.assert_array_less(np.abs(eig[4 * s:4 * s + 4] - t), RTOL * np.abs(t))
+        np.testing.assert_allclose(det[s], np.prod(t), rtol=1e-4)
+
+
+def test_dropin_example3_shape():
+    # example3.cu: subset {0..7} repeated, subIndexLen 256, minor 8
+    g, fx = _fixture()
+    sub = np.tile(np.arange(8, dtype=np.int32), 32)
+    eig = np.zeros(256)
+    det = np.zeros(32)
+    assert api.calculate_subeigs3(g.copy(), 256, 8, eig, det, sub, 8) == 0
+    t = np.array(fx["cases"][1]["dsyev_eigs"])
+    for s in range(32):
+        np.testing.assert_array_less(np.abs(eig[8 * s:8 * s + 8] - t), RTOL * np.abs(t))
+
+
+def test_dropin_example1_and_calculate_eigs():
+    g, fx = _fixture()
+    eig = np.zeros(8)
+    det = np.zeros(1)
+    assert api.calculate_subeigs(g.copy(), 8, eig, det, np.array([1, 3, 5, 7], np.int32), 4) == 0
+    t = np.array(fx["cases"][0]["dsyev_eigs"])
+    np.testing.assert_array_less(np.abs(eig[:4] - t), RTOL * np.abs(t))
+    np.testing.assert_allclose(det[0], np.prod(t), rtol=1e-4)
+    assert api.calculate_eigs(g.copy(), 8, eig, det) == 0
+    t = np.array(fx["cases"][1]["dsyev_eigs"])
+    np.testing.assert_array_less(np.abs(eig - t), RTOL * np.abs(t))
+
+
+def test_dropin_ragged_tail_is_solved():
+    # the reference's grid of subIndexLen/128 blocks skips sets past the last
+    # full block; every set is solved here
+    g, fx = _fixture()
+    sub = np.tile(np.array([1, 3, 5, 7], np.int32), 40)  # 160 indices, 40 sets
+    eig = np.zeros(160)
+    det = np.zeros(40)
+    assert api.calculate_subeigs3(g.copy(), 160, 8, eig, det, sub, 4) == 0
+    t = np.array(fx["cases"][0]["dsyev_eigs"])
+    np.testing.assert_array_less(np.abs(eig[-4:] - t), RTOL * np.abs(t))
+
+
+# ----------------------------------------------------------------------------- edge cases
+
+
+def test_bad_indices_and_k_reported_per_set():
+    A = cached_gram(256, 512)
+    idx = np.array([0, 1, 2, 3, 5, -1, 7, 8, 9, 10, 11, 512], np.int32)
+    res = run(A, idx, k=4)
+    assert res["err"][0] == 0
+    assert res["err"][1] & _lib.PL_SET_BAD_INDEX and np.isnan(res["lmin"][1])
+    assert res["err"][2] & _lib.PL_SET_BAD_INDEX and np.isnan(res["lmax"][2])
+    offs = np.array([0, 4, 4 + 600], np.int64)
+    idx2 = np.r_[np.arange(4), np.arange(600) % 512].astype(np.int32)
+    res = run(cached_gram(256, 1024), idx2, offsets=offs)
+    assert res["err"][0] == 0 and res["err"][1] & _lib.PL_SET_BAD_K
+
+
+def test_nonfinite_input():
+    A = np.eye(16, dtype=np.float32) * 2
+    A[3, 3] = np.nan
+    res = run(A, np.arange(16, dtype=np.int32), k=16)
+    assert res["err"][0] & _lib.PL_SET_NONFINITE and np.isnan(res["lmin"][0])
+
+
+@pytest.mark.parametrize("k", [8, 16, 40, 64, 100, 200])
+def test_breakdown_restart(k):
+    # A = I and a block-diagonal matrix: the all-ones start vector spans an
+    # invariant subspace after one step (the reference divides by beta = 0)
+    for A in (np.eye(k, dtype=np.float32),
+              np.kron(np.eye(2), np.ones((k // 2, k // 2))).astype(np.float32) + np.eye(k, dtype=np.float32)):
+        res = run(A, np.arange(k, dtype=np.int32), k=k, want_all=True)
+        t = np.linalg.eigvalsh(A.astype(np.float64))
+        assert res["err"][0] & _lib.PL_SET_BREAKDOWN
+        np.testing.assert_allclose(res["eig"], t, rtol=RTOL, atol=1e-6)
+
+
+def test_singular_and_duplicate_indices():
+    A = cached_gram(64, 256)  # rank 64: sets of k > 64 are singular
+    k = 96
+    o, idx = O.gen_stream(8, 0, 4, 256, 0, k, k)
+    res = run(A, idx, k=k, want_all=True)
+    truth = O.dsyev_batch(A, idx, k=k)
+    for s, t in enumerate(truth):
+        assert abs(res["lmax"][s] - t[-1]) <= RTOL * t[-1]
+        assert abs(res["lmin"][s]) < 1e-5 * t[-1]
+    dup = np.array([3, 3, 5, 9] * 1, np.int32)
+    res = run(A, dup, k=4)
+    assert abs(res["lmin"][0]) < 1e-6 and res["err"][0] in (0, _lib.PL_SET_BREAKDOWN)
+
+
+def test_k_one_and_k_equals_n():
+    A = cached_gram(256, 512)
+    res = run(A, np.array([5, 17, 300], np.int32), k=1)
+    np.testing.assert_allclose(res["lmin"], A[[5, 17, 300], [5, 17, 300]], rtol=1e-7)
+    B = cached_gram(256, 128)
+    res = run(B, np.arange(128, dtype=np.int32), k=128, want_all=True)
+    t = np.linalg.eigvalsh(B.astype(np.float64))
+    np.testing.assert_array_less(np.abs(res["eig"] - t), RTOL * np.abs(t))
+
+
+def test_empty_batch():
+    torch = _torch()
+    out = api.solve(dev(cached_gram(64, 128)), torch.zeros(0, dtype=torch.int32, device="cuda"), k=8)
+    assert out["lmin"].numel() == 0
+
+
+def test_result_independent_of_batch_composition():
+    A = cached_gram(1024, 4096)
+    offs, idx = O.gen_stream(12, 0, 400, 4096, 1, 8, 256)
+    mix = run(A, idx, offsets=offs)
+    for s in (0, 7, 123, 399):
+        S = idx[offs[s]:offs[s + 1]]
+        alone = run(A, S, k=len(S))
+        assert alone["lmin"][0] == mix["lmin"][s] and alone["lmax"][0] == mix["lmax"][s]
+
+
+def test_device_generator_matches_host():
+    torch = _torch()
+    for (n, k, first) in [(512, 16, 0), (4096, 64, 1000), (300, 300, 5)]:
+        d = api.gen_sets(9, first, 500, n, k).cpu().numpy()
+        o, h = O.gen_stream(9, first, 500, n, 0, k, k)
+        np.testing.assert_array_equal(d, h)
+
+
+def test_solve_host_equals_device():
+    A = cached_gram(1024, 4096)
+    offs, idx = O.gen_stream(13, 0, 300, 4096, 1, 8, 256)
+    h = api.solve_host(A, idx, offsets=offs)
+    d = run(A, idx, offsets=offs)
+    for n in ("lmin", "lmax", "delta", "err"):
+        np.testing.assert_array_equal(h[n], d[n])
+    o2, idx2 = O.gen_stream(13, 0, 300, 4096, 0, 64, 64)
+    h = api.solve_host(A, idx2, k=64, want_all=True)
+    d = run(A, idx2, k=64, want_all=True)
+    for n in ("lmin", "lmax", "eig", "det"):
+        np.testing.assert_array_equal(h[n], d[n])
+
+
+def test_tuning_variants_agree():
+    A = cached_gram(1024, 4096)
+    for b in range(api.num_bins()):
+        kmax = api.bin_kmax(b)
+        if kmax > 128:
+            continue
+        k = kmax
+        o, idx = O.gen_stream(14, 0, 64, 4096, 0, k, k)
+        nvar, _ = api.tune_describe(b, 0)
+        outs = []
+        for v in range(nvar):
+            api.tune_set(b, v)
+            outs.append(run(A, idx, k=k))
+        api.tune_set(b, -1)
+        truth = O.dsyev_batch(A, idx, k=k)
+        for r in outs:
+            for s, t in enumerate(truth):
+                assert abs(r["lmin"][s] - t[0]) <= RTOL * t[0]
+                assert abs(r["lmax"][s] - t[-1]) <= RTOL * t[-1]
