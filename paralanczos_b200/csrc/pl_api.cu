@@ -45,8 +45,12 @@ int device_sms() {
   return sms[dev] > 0 ? sms[dev] : 148;
 }
 
+// nitems < 0: the item count lives on the device.  prep: only load the kernel
+// and cache its launch attributes (done before a stream capture starts).
 typedef cudaError_t (*LaunchFn)(const MatrixF32&, const SetSource&, const SetOutputs&, long long,
-                                float*, cudaStream_t);
+                                void*, cudaStream_t, bool prep);
+// Bytes of device scratch a variant needs at its full (persistent) grid.
+typedef size_t (*ScratchFn)();
 
 template <class K>
 int occupancy(K kern, int cta, size_t dsmem) {
@@ -64,18 +68,64 @@ long long grid_for(long long nitems, int per_cta, int occ) {
 
 template <int KB, int RPT, int TPR, int CTA, int MINB, bool ALL>
 cudaError_t launch_reg(const MatrixF32& M, const SetSource& src, const SetOutputs& out,
-                       long long nitems, float*, cudaStream_t st) {
+                       long long nitems, void* scratch, cudaStream_t st, bool prep) {
   auto kern = k_reg_solve<KB, RPT, TPR, CTA, MINB, ALL>;
   static int occ = occupancy(kern, CTA, 0);
+  if (prep) {
+    cudaFuncAttributes fa;
+    return cudaFuncGetAttributes(&fa, kern);
+  }
   constexpr int GPC = CTA / Cfg<KB, RPT, TPR>::NT;
   const long long grid = grid_for(nitems, GPC, occ);
-  kern<<<(unsigned)grid, CTA, 0, st>>>(M, src, out);
+  kern<<<(unsigned)grid, CTA, 0, st>>>(M, src, out, (double2*)scratch);
   return cudaGetLastError();
+}
+
+// Queue buffer of the deferred bisection: per group Q = NT/2 tridiagonals of KB.
+template <int KB, int RPT, int TPR, int CTA, int MINB, bool ALL>
+size_t scratch_reg() {
+  if (ALL) return 0;
+  auto kern = k_reg_solve<KB, RPT, TPR, CTA, MINB, ALL>;
+  constexpr int NT = Cfg<KB, RPT, TPR>::NT;
+  const size_t grid = (size_t)device_sms() * occupancy(kern, CTA, 0);
+  return grid * (CTA / NT) * (NT / 2) * KB * sizeof(double2);
+}
+
+template <int KB, int RPT, int CTA, int MINB, bool ALL>
+cudaError_t launch_sa(const MatrixF32& M, const SetSource& src, const SetOutputs& out,
+                      long long nitems, void* scratch, cudaStream_t st, bool prep) {
+  auto kern = k_sa_solve<KB, RPT, CTA, MINB, ALL>;
+  constexpr int GPC = CTA / CfgSA<KB, RPT>::NT;
+  const size_t dsm = sizeof(SASmem<KB, RPT>) * GPC;
+  static int occ = [&] {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
+    cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    return occupancy(kern, CTA, dsm);
+  }();
+  if (prep) {
+    cudaFuncAttributes fa;
+    return cudaFuncGetAttributes(&fa, kern);
+  }
+  const long long grid = grid_for(nitems, GPC, occ);
+  kern<<<(unsigned)grid, CTA, dsm, st>>>(M, src, out, (double2*)scratch);
+  return cudaGetLastError();
+}
+
+template <int KB, int RPT, int CTA, int MINB, bool ALL>
+size_t scratch_sa() {
+  if (ALL) return 0;
+  auto kern = k_sa_solve<KB, RPT, CTA, MINB, ALL>;
+  constexpr int NT = CfgSA<KB, RPT>::NT;
+  const size_t dsm = sizeof(SASmem<KB, RPT>) * (CTA / NT);
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
+  cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  const size_t grid = (size_t)device_sms() * occupancy(kern, CTA, dsm);
+  return grid * (CTA / NT) * (NT / 2) * KB * sizeof(double2);
 }
 
 template <int KB, bool ALL>
 cudaError_t launch_plain(const MatrixF32& M, const SetSource& src, const SetOutputs& out,
-                         long long nitems, float*, cudaStream_t st) {
+                         long long nitems, void*, cudaStream_t st, bool prep) {
   constexpr int NT = KB < 32 ? 32 : KB;
   const size_t dsm = sizeof(float) * 2 * KB * (KB + 1);
   auto kern = k_plain<KB, ALL>;
@@ -84,6 +134,10 @@ cudaError_t launch_plain(const MatrixF32& M, const SetSource& src, const SetOutp
     return true;
   }();
   (void)attr;
+  if (prep) {
+    cudaFuncAttributes fa;
+    return cudaFuncGetAttributes(&fa, kern);
+  }
   // one set per thread block; grid-stride only beyond the grid limit
   long long grid = nitems < 0 ? (long long)device_sms() * 16 : nitems;
   if (grid > 0x7fffffffLL) grid = 0x7fffffffLL;
@@ -94,39 +148,57 @@ cudaError_t launch_plain(const MatrixF32& M, const SetSource& src, const SetOutp
 
 template <int KM, bool ALL>
 cudaError_t launch_large(const MatrixF32& M, const SetSource& src, const SetOutputs& out,
-                         long long nitems, float* scratch, cudaStream_t st) {
+                         long long nitems, void* scratch, cudaStream_t st, bool prep) {
   auto kern = k_large<KM, ALL>;
+  if (prep) {
+    cudaFuncAttributes fa;
+    return cudaFuncGetAttributes(&fa, kern);
+  }
   const long long grid = grid_for(nitems, 1, 1);
-  kern<<<(unsigned)grid, 256, 0, st>>>(M, src, out, scratch);
+  kern<<<(unsigned)grid, 256, 0, st>>>(M, src, out, (float*)scratch);
   return cudaGetLastError();
 }
 
+template <int KM>
+size_t scratch_large() {
+  return sizeof(float) * 2 * (size_t)KM * KM * (size_t)device_sms();
+}
+size_t scratch_none() { return 0; }
+
 struct Variant {
   const char* desc;
-  LaunchFn fn[2];  // [extremes only, all eigenvalues]
-  bool large;      // needs the scratch slots
-  int km;          // scratch k capacity (large only)
+  LaunchFn fn[2];       // [extremes only, all eigenvalues]
+  ScratchFn scratch[2]; // device scratch at the full grid
 };
 
 #define REG(KB, RPT, TPR, CTA, MINB)                                                          \
   Variant {                                                                                    \
     "reg KB=" #KB " RPT=" #RPT " TPR=" #TPR " CTA=" #CTA " MINB=" #MINB,                       \
         {launch_reg<KB, RPT, TPR, CTA, MINB, false>, launch_reg<KB, RPT, TPR, CTA, MINB, true>}, \
-        false, 0                                                                               \
+        {scratch_reg<KB, RPT, TPR, CTA, MINB, false>, scratch_none}                            \
+  }
+#define SA(KB, RPT, CTA, MINB)                                                               \
+  Variant {                                                                                    \
+    "sharedA KB=" #KB " RPT=" #RPT " CTA=" #CTA " MINB=" #MINB,                                \
+        {launch_sa<KB, RPT, CTA, MINB, false>, launch_sa<KB, RPT, CTA, MINB, true>},          \
+        {scratch_sa<KB, RPT, CTA, MINB, false>, scratch_none}                                  \
   }
 #define LARGE(KM) \
-  Variant { "large KM=" #KM " CTA=256", {launch_large<KM, false>, launch_large<KM, true>}, true, KM }
+  Variant {                                                                             \
+    "large KM=" #KM " CTA=256", {launch_large<KM, false>, launch_large<KM, true>},      \
+        {scratch_large<KM>, scratch_large<KM>}                                           \
+  }
 
 const int kBinK[] = {8, 16, 32, 64, 128, 256, 512};
 constexpr int kNumBins = 7;
 
 const std::vector<Variant>& variants(int b) {
   static const std::vector<Variant> v[kNumBins] = {
-      {REG(8, 1, 1, 128, 4), REG(8, 2, 1, 128, 4), REG(8, 1, 1, 256, 4)},
-      {REG(16, 1, 1, 128, 4), REG(16, 2, 1, 128, 4), REG(16, 1, 1, 256, 3)},
-      {REG(32, 1, 1, 128, 4), REG(32, 2, 1, 128, 3), REG(32, 1, 2, 128, 4)},
-      {REG(64, 1, 1, 128, 3), REG(64, 1, 2, 128, 3), REG(64, 1, 1, 64, 6), REG(64, 1, 1, 256, 1)},
-      {REG(128, 1, 2, 256, 1)},
+      {REG(8, 2, 1, 128, 4), REG(8, 1, 1, 128, 4), SA(8, 2, 128, 4)},
+      {REG(16, 2, 1, 128, 4), REG(16, 1, 1, 128, 4), SA(16, 2, 128, 4)},
+      {REG(32, 2, 1, 128, 3), REG(32, 1, 1, 128, 4), SA(32, 2, 128, 4)},
+      {REG(64, 1, 1, 128, 3), SA(64, 2, 128, 3), REG(64, 1, 1, 128, 2), SA(64, 2, 128, 2)},
+      {SA(128, 1, 128, 3), REG(128, 1, 2, 256, 1), SA(128, 1, 128, 2)},
       {LARGE(256)},
       {LARGE(512)},
   };
@@ -170,6 +242,7 @@ struct DevState {
   DevScratch bins;     // counts / starts / cursor / perm
   DevScratch upload;   // pl_solve_host and drop-in staging
   cudaStream_t side[kNumBins] = {};
+  cudaStream_t cap = nullptr;  // private stream the CSR graph is captured on
   cudaEvent_t ev_fork = nullptr;
   cudaEvent_t ev_join[kNumBins] = {};
   struct GraphEntry {
@@ -211,6 +284,7 @@ int ensure(DevScratch& s, size_t bytes) {
 int ensure_streams(DevState& d) {
   if (d.ev_fork) return PL_OK;
   PL_CU(cudaEventCreateWithFlags(&d.ev_fork, cudaEventDisableTiming));
+  PL_CU(cudaStreamCreateWithFlags(&d.cap, cudaStreamNonBlocking));
   for (int b = 0; b < kNumBins; ++b) {
     PL_CU(cudaStreamCreateWithFlags(&d.side[b], cudaStreamNonBlocking));
     PL_CU(cudaEventCreateWithFlags(&d.ev_join[b], cudaEventDisableTiming));
@@ -230,20 +304,20 @@ int solve_uniform(const MatrixF32& M, const int* idx, long long nsets, int k, in
   const bool all = out.eig || out.det;
   SetSource src{idx, nullptr, k, nullptr, nullptr, nullptr, nsets};
   if (form == PL_FORM_PLAIN && k <= 128) {
-    PL_CU(plain_fn(k, all)(M, src, out, nsets, nullptr, st));
+    PL_CU(plain_fn(k, all)(M, src, out, nsets, nullptr, st, false));
     return PL_OK;
   }
   const int b = bin_of_k(k);
   if (b < 0) return PL_ENOTSUP;
   const Variant& v = chosen(b);
-  float* scratch = nullptr;
-  if (v.large) {
-    const long long slots = grid_for(nsets, 1, 1);
-    int rc = ensure(state().large, sizeof(float) * 2 * (size_t)v.km * v.km * (size_t)slots);
+  void* scratch = nullptr;
+  const size_t need = v.scratch[all ? 1 : 0]();
+  if (need) {
+    int rc = ensure(state().large, need);
     if (rc) return rc;
-    scratch = (float*)state().large.p;
+    scratch = state().large.p;
   }
-  PL_CU(v.fn[all ? 1 : 0](M, src, out, nsets, scratch, st));
+  PL_CU(v.fn[all ? 1 : 0](M, src, out, nsets, scratch, st, false));
   return PL_OK;
 }
 
@@ -260,22 +334,23 @@ int solve_csr(const MatrixF32& M, const int* idx, const long long* offsets, long
   const size_t hdr = 3 * 16;  // counts / starts / cursor, 16 ints each
   rc = ensure(d.bins, sizeof(int) * (hdr + (size_t)nsets));
   if (rc) return rc;
-  // every large-k bin gets its own scratch region: the bins run concurrently
-  const long long slots = device_sms();
+  // every bin gets its own scratch region: the bins run concurrently
   size_t large_off[kNumBins] = {0};
   size_t large_total = 0;
   for (int b = 0; b < nb; ++b) {
     large_off[b] = large_total;
-    if (chosen(b).large) large_total += 2 * (size_t)chosen(b).km * chosen(b).km * (size_t)slots;
+    const bool plain_bin = form == PL_FORM_PLAIN && kBinK[b] <= 128;
+    const size_t need = plain_bin ? 0 : chosen(b).scratch[all ? 1 : 0]();
+    large_total += (need + 255) & ~(size_t)255;
   }
-  rc = ensure(d.large, sizeof(float) * (large_total > 0 ? large_total : 1));
+  rc = ensure(d.large, large_total > 0 ? large_total : 256);
   if (rc) return rc;
   char keybuf[512];
-  snprintf(keybuf, sizeof keybuf, "%p|%d|%lld|%p|%p|%lld|%d|%p|%p|%p|%p|%p|%p|%p|%d%d%d%d%d%d%d",
+  snprintf(keybuf, sizeof keybuf, "%p|%d|%lld|%p|%p|%lld|%d|%p|%p|%p|%p|%p|%p|%d%d%d%d%d%d%d",
            (const void*)M.A, M.n, M.lda, (const void*)idx, (const void*)offsets, nsets, form,
            (void*)out.lmin, (void*)out.lmax, (void*)out.delta, (void*)out.err, (void*)out.eig,
-           (void*)out.det, (void*)st, g_variant[0], g_variant[1], g_variant[2], g_variant[3],
-           g_variant[4], g_variant[5], g_variant[6]);
+           (void*)out.det, g_variant[0], g_variant[1], g_variant[2], g_variant[3], g_variant[4],
+           g_variant[5], g_variant[6]);
   const std::string key(keybuf);
   auto it = d.graphs.find(key);
   if (it == d.graphs.end()) {
@@ -286,47 +361,52 @@ int solve_csr(const MatrixF32& M, const int* idx, const long long* offsets, long
     BinTable bt;
     bt.nb = nb;
     for (int b = 0; b < nb; ++b) bt.kmax[b] = kBinK[b];
-    cudaStream_t cs = st;
-    cudaStreamCaptureStatus cst;
-    PL_CU(cudaStreamIsCapturing(cs, &cst));
-    if (cst != cudaStreamCaptureStatusNone) return PL_EINVAL;
+    LaunchFn fns[kNumBins];
+    for (int b = 0; b < nb; ++b) {
+      fns[b] = (form == PL_FORM_PLAIN && kBinK[b] <= 128) ? plain_fn(kBinK[b], all)
+                                                          : chosen(b).fn[all ? 1 : 0];
+      // load every kernel before the capture: nothing that may load a module
+      // or set a function attribute runs while the stream is capturing
+      PL_CU(fns[b](M, SetSource{}, out, 0, nullptr, d.side[b], true));
+    }
+    cudaStream_t cs = d.cap;  // graphs do not depend on the stream they were captured on
     PL_CU(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    cudaMemsetAsync(counts, 0, sizeof(int) * 16, cs);
+    cudaError_t e = cudaSuccess;
+    auto note = [&](cudaError_t x) {
+      if (e == cudaSuccess && x != cudaSuccess) e = x;
+    };
+    note(cudaMemsetAsync(counts, 0, sizeof(int) * 16, cs));
     const int tb = 256;
     const long long g = (nsets + tb - 1) / tb;
     const unsigned grid = (unsigned)(g < 4096 ? (g > 0 ? g : 1) : 4096);
     k_bin_count<<<grid, tb, 0, cs>>>(offsets, nsets, bt, counts);
+    note(cudaGetLastError());
     k_bin_scan<<<1, 32, 0, cs>>>(counts, nb, starts, cursor);
+    note(cudaGetLastError());
     k_bin_scatter<<<grid, tb, 0, cs>>>(offsets, nsets, bt, starts, cursor, perm);
+    note(cudaGetLastError());
     k_mark_bad_k<<<64, 256, 0, cs>>>(perm, starts + nb, counts + nb, offsets, out);
-    cudaEventRecord(d.ev_fork, cs);
+    note(cudaGetLastError());
+    note(cudaEventRecord(d.ev_fork, cs));
     // largest-k bins first so the small-k kernels fill the tail
-    for (int b = nb - 1; b >= 0; --b) {
-      cudaStreamWaitEvent(d.side[b], d.ev_fork, 0);
+    for (int b = nb - 1; b >= 0 && e == cudaSuccess; --b) {
+      note(cudaStreamWaitEvent(d.side[b], d.ev_fork, 0));
       SetSource src{idx, offsets, 0, perm, starts + b, counts + b, 0};
-      cudaError_t e;
-      if (form == PL_FORM_PLAIN && kBinK[b] <= 128) {
-        e = plain_fn(kBinK[b], all)(M, src, out, -1, nullptr, d.side[b]);
-      } else {
-        const Variant& v = chosen(b);
-        e = v.fn[all ? 1 : 0](M, src, out, -1, (float*)d.large.p + large_off[b], d.side[b]);
-      }
-      if (e != cudaSuccess) {
-        cudaGraph_t gr;
-        cudaStreamEndCapture(cs, &gr);
-        if (gr) cudaGraphDestroy(gr);
-        g_last_cuda = (int)e;
-        return PL_ECUDA;
-      }
-      cudaEventRecord(d.ev_join[b], d.side[b]);
-      cudaStreamWaitEvent(cs, d.ev_join[b], 0);
+      note(fns[b](M, src, out, -1, (char*)d.large.p + large_off[b], d.side[b], false));
+      note(cudaEventRecord(d.ev_join[b], d.side[b]));
+      note(cudaStreamWaitEvent(cs, d.ev_join[b], 0));
     }
     cudaGraph_t graph = nullptr;
-    PL_CU(cudaStreamEndCapture(cs, &graph));
+    note(cudaStreamEndCapture(cs, &graph));  // always ends the capture
     cudaGraphExec_t exec = nullptr;
-    cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
-    cudaGraphDestroy(graph);
-    PL_CU(e);
+    if (e == cudaSuccess) note(cudaGraphInstantiate(&exec, graph, 0));
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      if (exec) cudaGraphExecDestroy(exec);
+      cudaGetLastError();
+      g_last_cuda = (int)e;
+      return PL_ECUDA;
+    }
     it = d.graphs.emplace(key, DevState::GraphEntry{exec}).first;
   }
   PL_CU(cudaGraphLaunch(it->second.exec, st));

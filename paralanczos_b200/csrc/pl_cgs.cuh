@@ -25,8 +25,7 @@ struct __align__(16) CgsSmem {
   float wb[KM];
   float hb[KM];
   int idx[KM];
-  double alpha[KM];
-  double beta2[KM + 1];
+  double2 ab[KM];  // T: ab[i] = {alpha_i, beta_i^2}
   double red[6][NW];
 };
 
@@ -146,20 +145,20 @@ __device__ __forceinline__ void cgs_solve_set(const MatrixF32& M, const int* __r
     }
     const double b2v = group_sum<NT, NW>(bp, g, sm.red[1]);
     if (t == 0) {
-      sm.alpha[j] = alpha;
-      if (j + 1 < k) sm.beta2[j + 1] = b2v;
+      sm.ab[j].x = alpha;
+      if (j + 1 < k) sm.ab[j + 1].y = b2v;
     }
     if (!isfinite(alpha) || !isfinite(b2v)) {
       status |= SET_NONFINITE;
       break;
     }
     if (j + 1 == k) break;
-    const double bet = sqrt(b2v);
 #pragma unroll
     for (int q = 0; q < RM; ++q) vp[q] = v[q];
-    if (bet > tau) {
-      const float inv = (float)(1.0 / bet);
-      bprev = (float)bet;
+    if (b2v > tau * tau) {
+      const float bf = sqrtf((float)b2v);
+      const float inv = 1.0f / bf;
+      bprev = bf;
 #pragma unroll
       for (int q = 0; q < RM; ++q) v[q] = w[q] * inv;
     } else {
@@ -197,8 +196,8 @@ __device__ __forceinline__ void cgs_solve_set(const MatrixF32& M, const int* __r
         }
       }
       const double zz = group_sum<NT, NW>(zp, g, sm.red[1]);
-      if (t == 0) sm.beta2[j + 1] = 0.0;
-      const float inv = (float)(1.0 / sqrt(zz));
+      if (t == 0) sm.ab[j + 1].y = 0x1p-600;  // decoupled block (see sturm_count)
+      const float inv = 1.0f / sqrtf((float)zz);
       bprev = 0.f;
 #pragma unroll
       for (int q = 0; q < RM; ++q) v[q] = w[q] * inv;
@@ -224,9 +223,9 @@ __device__ __forceinline__ void cgs_solve_set(const MatrixF32& M, const int* __r
 
   double glo = 1e300, ghi = -1e300;
   for (int i = t; i < k; i += NT) {
-    const double rad = (i > 0 ? sqrt(sm.beta2[i]) : 0.0) + (i + 1 < k ? sqrt(sm.beta2[i + 1]) : 0.0);
-    glo = fmin(glo, sm.alpha[i] - rad);
-    ghi = fmax(ghi, sm.alpha[i] + rad);
+    const double rad = (i > 0 ? sqrt(sm.ab[i].y) : 0.0) + (i + 1 < k ? sqrt(sm.ab[i + 1].y) : 0.0);
+    glo = fmin(glo, sm.ab[i].x - rad);
+    ghi = fmax(ghi, sm.ab[i].x + rad);
   }
   glo = group_minmax<NT, NW, false>(glo, g, sm.red[2]);
   ghi = group_minmax<NT, NW, true>(ghi, g, sm.red[3]);
@@ -236,12 +235,26 @@ __device__ __forceinline__ void cgs_solve_set(const MatrixF32& M, const int* __r
     ghi += pad;
   }
   if constexpr (!ALL) {
-    if (g.wig == 0) {
+    if constexpr (NW >= 2) {
+      // warp 0 brackets lambda_min, warp 1 lambda_max, 33-way each
+      if (g.wig < 2) {
+        const double e = multisect_warp(sm.ab, k, glo, ghi, g.wig == 0 ? 1 : k);
+        if ((threadIdx.x & 31) == 0) sm.red[4 + g.wig][0] = e;
+      }
+      g.sync();
+      if (t == 0) {
+        const double lmin = sm.red[4][0], lmax = sm.red[5][0];
+        if (out.lmin) out.lmin[set] = lmin;
+        if (out.lmax) out.lmax[set] = lmax;
+        if (out.delta) out.delta[set] = fmax(1.0 - lmin, lmax - 1.0);
+        if (out.err) out.err[set] = status;
+      }
+    } else {
       constexpr int GW = NT < 32 ? NT : 32;
       const int base = (NT < 32) ? ((threadIdx.x & 31) / NT) * NT : 0;
       const unsigned mask = (NT < 32) ? g.mask : 0xffffffffu;
       double lmin, lmax;
-      multisect_extremes(sm.alpha, sm.beta2, k, glo, ghi, GW / 2, base, mask, lmin, lmax);
+      multisect_extremes(sm.ab, k, glo, ghi, GW / 2, base, mask, lmin, lmax);
       if (t == 0) {
         if (out.lmin) out.lmin[set] = lmin;
         if (out.lmax) out.lmax[set] = lmax;
@@ -260,7 +273,7 @@ __device__ __forceinline__ void cgs_solve_set(const MatrixF32& M, const int* __r
     }
     double prod = 1.0;
     for (int m = t; m < k; m += NT) {
-      const double e = bisect_index(sm.alpha, sm.beta2, k, m, glo, ghi, R);
+      const double e = bisect_index(sm.ab, k, m, glo, ghi, R);
       if (out.eig) out.eig[off + m] = e;
       prod *= e;
       if (m == 0) {

@@ -46,8 +46,7 @@ struct __align__(16) GroupSmem {
   float vb[KB];         // broadcast of the (unnormalised) next Lanczos vector
   float wb[KB];         // broadcast of the three-term residual w~
   int idx[KB];          // the set's indices
-  double alpha[KB];     // T diagonal
-  double beta2[KB + 1]; // beta2[i] = beta_i^2 couples rows i-1, i
+  double2 ab[KB];       // T: ab[i] = {alpha_i, beta_i^2}, beta_i couples rows i-1, i
   double red[6][NW];    // cross-warp partials (slots 4/5: lambda_min/max hand-off)
 };
 
@@ -173,7 +172,7 @@ __device__ __forceinline__ void write_failed(const SetOutputs& out, long long se
 
 // Solve one set with the calling group.  S: the set's k indices (global).
 template <int KB, int RPT, int TPR, bool ALL>
-__device__ __forceinline__ void solve_set(const MatrixF32& M, const int* __restrict__ S, int k,
+__device__ __forceinline__ int solve_set(const MatrixF32& M, const int* __restrict__ S, int k,
                                           long long set, long long off, const SetOutputs& out,
                                           GroupSmem<KB, Cfg<KB, RPT, TPR>::NW>& sm,
                                           const Grp<Cfg<KB, RPT, TPR>::NT>& g) {
@@ -199,13 +198,14 @@ __device__ __forceinline__ void solve_set(const MatrixF32& M, const int* __restr
   if (group_any<NT, NW>(bad, g, sm.red[3])) {
     if (t == 0) write_failed(out, set, off, ALL ? k : 0, SET_BAD_INDEX);
     g.sync();
-    return;
+    return -1;
   }
   g.sync();
 
   // ---- gather A[S,S] rows into registers; P = I ------------------------------
-  float Ar[RPT][CPT];
-  float Pr[RPT][CPT];
+  // rows stored as column pairs: packed FP32 (FFMA2) halves the FMA issues
+  float2 Ar[RPT][CPT / 2];
+  float2 Pr[RPT][CPT / 2];
   int rowid[RPT];
   double fro = 0.0;
 #pragma unroll
@@ -215,13 +215,13 @@ __device__ __forceinline__ void solve_set(const MatrixF32& M, const int* __restr
     const bool rv = r < k;
     const float* __restrict__ arow = M.A + (size_t)sm.idx[r] * (size_t)M.lda;
 #pragma unroll
-    for (int cc = 0; cc < CPT; ++cc) {
+    for (int cc = 0; cc < CPT; cc += 2) {
       const int c = c0 + cc;
-      float a = 0.f;
-      if (rv && c < k) a = __ldg(arow + sm.idx[c]);
-      Ar[q][cc] = a;
-      Pr[q][cc] = (rv && c == r) ? 1.f : 0.f;
-      fro += (double)a * (double)a;
+      const float a0 = (rv && c < k) ? __ldg(arow + sm.idx[c]) : 0.f;
+      const float a1 = (rv && c + 1 < k) ? __ldg(arow + sm.idx[c + 1]) : 0.f;
+      Ar[q][cc / 2] = make_float2(a0, a1);
+      Pr[q][cc / 2] = make_float2((rv && c == r) ? 1.f : 0.f, (rv && c + 1 == r) ? 1.f : 0.f);
+      fro += (double)a0 * (double)a0 + (double)a1 * (double)a1;
     }
   }
   const double fro2 = group_sum<NT, NW>(fro, g, sm.red[2]);
@@ -243,32 +243,31 @@ __device__ __forceinline__ void solve_set(const MatrixF32& M, const int* __restr
 
   for (int j = 0; j < k; ++j) {
     // P -= v v^T and y = A v, one pass over the broadcast vector
-    float y[RPT], y2[RPT], coef[RPT];
+    float2 ya[RPT], yb[RPT], ncoef[RPT];
 #pragma unroll
     for (int q = 0; q < RPT; ++q) {
-      y[q] = 0.f;
-      y2[q] = 0.f;
-      coef[q] = v[q] * sc;
+      ya[q] = make_float2(0.f, 0.f);
+      yb[q] = make_float2(0.f, 0.f);
+      const float cq = -v[q] * sc;
+      ncoef[q] = make_float2(cq, cq);
     }
 #pragma unroll
     for (int cc = 0; cc < CPT; cc += 4) {
       const float4 b4 = *reinterpret_cast<const float4*>(&sm.vb[c0 + cc]);
+      const float2 b01 = make_float2(b4.x, b4.y), b23 = make_float2(b4.z, b4.w);
 #pragma unroll
       for (int q = 0; q < RPT; ++q) {
-        Pr[q][cc + 0] = fmaf(-coef[q], b4.x, Pr[q][cc + 0]);
-        Pr[q][cc + 1] = fmaf(-coef[q], b4.y, Pr[q][cc + 1]);
-        Pr[q][cc + 2] = fmaf(-coef[q], b4.z, Pr[q][cc + 2]);
-        Pr[q][cc + 3] = fmaf(-coef[q], b4.w, Pr[q][cc + 3]);
-        y[q] = fmaf(Ar[q][cc + 0], b4.x, y[q]);
-        y2[q] = fmaf(Ar[q][cc + 1], b4.y, y2[q]);
-        y[q] = fmaf(Ar[q][cc + 2], b4.z, y[q]);
-        y2[q] = fmaf(Ar[q][cc + 3], b4.w, y2[q]);
+        Pr[q][cc / 2] = __ffma2_rn(ncoef[q], b01, Pr[q][cc / 2]);
+        Pr[q][cc / 2 + 1] = __ffma2_rn(ncoef[q], b23, Pr[q][cc / 2 + 1]);
+        ya[q] = __ffma2_rn(Ar[q][cc / 2], b01, ya[q]);
+        yb[q] = __ffma2_rn(Ar[q][cc / 2 + 1], b23, yb[q]);
       }
     }
+    float y[RPT];
     double ap = 0.0;
 #pragma unroll
     for (int q = 0; q < RPT; ++q) {
-      y[q] = (y[q] + y2[q]) * sc;
+      y[q] = ((ya[q].x + ya[q].y) + (yb[q].x + yb[q].y)) * sc;
       if constexpr (TPR == 2) y[q] += __shfl_xor_sync(g.mask, y[q], 1);
       if (lead) ap += (double)v[q] * (double)y[q];
     }
@@ -285,27 +284,27 @@ __device__ __forceinline__ void solve_set(const MatrixF32& M, const int* __restr
     g.sync();
 
     // w = P w~
-    float w[RPT], w2[RPT];
+    float2 wa[RPT], wb2[RPT];
 #pragma unroll
     for (int q = 0; q < RPT; ++q) {
-      w[q] = 0.f;
-      w2[q] = 0.f;
+      wa[q] = make_float2(0.f, 0.f);
+      wb2[q] = make_float2(0.f, 0.f);
     }
 #pragma unroll
     for (int cc = 0; cc < CPT; cc += 4) {
       const float4 x4 = *reinterpret_cast<const float4*>(&sm.wb[c0 + cc]);
+      const float2 x01 = make_float2(x4.x, x4.y), x23 = make_float2(x4.z, x4.w);
 #pragma unroll
       for (int q = 0; q < RPT; ++q) {
-        w[q] = fmaf(Pr[q][cc + 0], x4.x, w[q]);
-        w2[q] = fmaf(Pr[q][cc + 1], x4.y, w2[q]);
-        w[q] = fmaf(Pr[q][cc + 2], x4.z, w[q]);
-        w2[q] = fmaf(Pr[q][cc + 3], x4.w, w2[q]);
+        wa[q] = __ffma2_rn(Pr[q][cc / 2], x01, wa[q]);
+        wb2[q] = __ffma2_rn(Pr[q][cc / 2 + 1], x23, wb2[q]);
       }
     }
+    float w[RPT];
     double bp = 0.0;
 #pragma unroll
     for (int q = 0; q < RPT; ++q) {
-      w[q] = w[q] + w2[q];
+      w[q] = (wa[q].x + wa[q].y) + (wb2[q].x + wb2[q].y);
       if constexpr (TPR == 2) w[q] += __shfl_xor_sync(g.mask, w[q], 1);
       if (lead) {
         bp += (double)w[q] * (double)w[q];
@@ -315,21 +314,21 @@ __device__ __forceinline__ void solve_set(const MatrixF32& M, const int* __restr
     const double b2v = group_sum<NT, NW>(bp, g, sm.red[1]);
     if constexpr (NW == 1) g.sync();
     if (t == 0) {
-      sm.alpha[j] = alpha;
-      if (j + 1 < k) sm.beta2[j + 1] = b2v;
+      sm.ab[j].x = alpha;
+      if (j + 1 < k) sm.ab[j + 1].y = b2v;
     }
     if (!isfinite(alpha) || !isfinite(b2v)) {
       status |= SET_NONFINITE;
       break;
     }
     if (j + 1 == k) break;
-    const double bet = sqrt(b2v);
 #pragma unroll
     for (int q = 0; q < RPT; ++q) vp[q] = v[q];
-    if (bet > tau) {
-      const float inv = (float)(1.0 / bet);
+    if (b2v > tau * tau) {
+      const float bf = sqrtf((float)b2v);
+      const float inv = 1.0f / bf;
       sc = inv;
-      bprev = (float)bet;
+      bprev = bf;
 #pragma unroll
       for (int q = 0; q < RPT; ++q) v[q] = w[q] * inv;
     } else {
@@ -343,8 +342,10 @@ __device__ __forceinline__ void solve_set(const MatrixF32& M, const int* __restr
         if (r < k && r >= c0 && r < c0 + CPT) {
           float d = 0.f;
 #pragma unroll
-          for (int cc = 0; cc < CPT; ++cc)
-            if (c0 + cc == r) d = Pr[q][cc];
+          for (int cc = 0; cc < CPT; cc += 2) {
+            if (c0 + cc == r) d = Pr[q][cc / 2].x;
+            if (c0 + cc + 1 == r) d = Pr[q][cc / 2].y;
+          }
           d = fmaxf(d, 0.f);
           const unsigned long long kk =
               ((unsigned long long)__float_as_uint(d) << 32) | (unsigned)(0x7fffffff - r);
@@ -358,7 +359,10 @@ __device__ __forceinline__ void solve_set(const MatrixF32& M, const int* __restr
       for (int q = 0; q < RPT; ++q)
         if (rowid[q] == m) {
 #pragma unroll
-          for (int cc = 0; cc < CPT; ++cc) sm.vb[c0 + cc] = Pr[q][cc];
+          for (int cc = 0; cc < CPT; cc += 2) {
+            sm.vb[c0 + cc] = Pr[q][cc / 2].x;
+            sm.vb[c0 + cc + 1] = Pr[q][cc / 2].y;
+          }
         }
       g.sync();
       double zp = 0.0;
@@ -369,8 +373,8 @@ __device__ __forceinline__ void solve_set(const MatrixF32& M, const int* __restr
         if (lead) zp += (double)z[q] * (double)z[q];
       }
       const double zz = group_sum<NT, NW>(zp, g, sm.red[1]);
-      if (t == 0) sm.beta2[j + 1] = 0.0;
-      const float inv = (float)(1.0 / sqrt(zz));
+      if (t == 0) sm.ab[j + 1].y = 0x1p-600;  // decoupled block (see sturm_count)
+      const float inv = 1.0f / sqrtf((float)zz);
       sc = inv;
       bprev = 0.f;
 #pragma unroll
@@ -379,18 +383,22 @@ __device__ __forceinline__ void solve_set(const MatrixF32& M, const int* __restr
   }
   g.sync();  // alpha / beta2 visible to every thread
 
+  if constexpr (!ALL) {
+    // extremes mode: T stays in sm.ab for the caller's deferred bisection
+    return status;
+  }
   if (status & SET_NONFINITE) {
     if (t == 0) write_failed(out, set, off, ALL ? k : 0, status);
     g.sync();
-    return;
+    return -1;
   }
 
   // ---- eigenvalues of T by FP64 Sturm bisection --------------------------------
   double glo = 1e300, ghi = -1e300;
   for (int i = t; i < k; i += NT) {
-    const double rad = (i > 0 ? sqrt(sm.beta2[i]) : 0.0) + (i + 1 < k ? sqrt(sm.beta2[i + 1]) : 0.0);
-    glo = fmin(glo, sm.alpha[i] - rad);
-    ghi = fmax(ghi, sm.alpha[i] + rad);
+    const double rad = (i > 0 ? sqrt(sm.ab[i].y) : 0.0) + (i + 1 < k ? sqrt(sm.ab[i + 1].y) : 0.0);
+    glo = fmin(glo, sm.ab[i].x - rad);
+    ghi = fmax(ghi, sm.ab[i].x + rad);
   }
   glo = group_minmax<NT, NW, false>(glo, g, sm.red[2]);
   ghi = group_minmax<NT, NW, true>(ghi, g, sm.red[3]);
@@ -400,22 +408,7 @@ __device__ __forceinline__ void solve_set(const MatrixF32& M, const int* __restr
     ghi += pad;
   }
 
-  if constexpr (!ALL) {
-    constexpr int GW = NT < 32 ? NT : 32;  // lanes that bisect: one warp
-    constexpr int G = GW / 2;
-    if (g.wig == 0) {
-      const int base = (NT < 32) ? ((threadIdx.x & 31) / NT) * NT : 0;
-      const unsigned mask = (NT < 32) ? g.mask : 0xffffffffu;
-      double lmin, lmax;
-      multisect_extremes(sm.alpha, sm.beta2, k, glo, ghi, G, base, mask, lmin, lmax);
-      if (t == 0) {
-        if (out.lmin) out.lmin[set] = lmin;
-        if (out.lmax) out.lmax[set] = lmax;
-        if (out.delta) out.delta[set] = fmax(1.0 - lmin, lmax - 1.0);
-        if (out.err) out.err[set] = status;
-      }
-    }
-  } else {
+  {
     int R = 0;
     {
       double wdt = ghi - glo, tol = bisect_tol(glo, ghi);
@@ -426,7 +419,7 @@ __device__ __forceinline__ void solve_set(const MatrixF32& M, const int* __restr
     }
     double prod = 1.0;
     for (int m = t; m < k; m += NT) {
-      const double e = bisect_index(sm.alpha, sm.beta2, k, m, glo, ghi, R);
+      const double e = bisect_index(sm.ab, k, m, glo, ghi, R);
       if (out.eig) out.eig[off + m] = e;
       prod *= e;
       if (m == 0 && out.lmin) out.lmin[set] = e;
@@ -458,6 +451,7 @@ __device__ __forceinline__ void solve_set(const MatrixF32& M, const int* __restr
     }
   }
   g.sync();
+  return -1;
 }
 
 }  // namespace pl

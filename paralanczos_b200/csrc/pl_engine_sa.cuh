@@ -1,0 +1,316 @@
+// pl_engine_sa.cuh -- "shared-A" per-set Lanczos: the projector P in
+// registers, A[S,S] in shared memory.
+//
+// Same recurrence as pl_engine.cuh (three-term step, then w = P w~ with the
+// explicit projector P = I - sum v v^T, P -= v v^T fused with the next matvec;
+// FP32 vectors, FP64 alpha/beta, FP64 Sturm multisection), but A_S is read
+// from shared memory instead of being held in registers.  That halves the
+// registers per set, so a k <= 64 set fits one warp (no named barriers, only
+// warp shuffles) and twice as many sets are in flight per SM, which is what
+// the latency-bound per-step chain y -> alpha -> w~ -> P w~ -> beta needs.
+//
+// A layout: thread t of a group of NT owns rows r_q = t + q*NT (q < RPT); its
+// row data is stored lane-interleaved, A[q][chunk][t][4] (4 floats per chunk),
+// so every thread's LDS.128 of its own row chunk is conflict-free and uses a
+// compile-time offset from one per-thread base pointer.
+#pragma once
+#include "pl_engine.cuh"
+
+namespace pl {
+
+template <int KB, int RPT>
+struct CfgSA {
+  static constexpr int NT = KB / RPT;  // threads per set
+  static constexpr int NCH = KB / 4;   // float4 chunks per row
+  static constexpr int NW = NT > 32 ? NT / 32 : 1;
+  static_assert(KB % RPT == 0 && KB % 4 == 0, "bad shape");
+  static_assert(NT <= 32 ? (32 % NT == 0) : (NT % 32 == 0), "bad group size");
+};
+
+template <int KB, int RPT>
+struct __align__(16) SASmem {
+  float4 A[RPT * (KB / 4) * (KB / RPT)];  // [q][chunk][thread] float4
+  float vb[KB];
+  float wb[KB];
+  int idx[KB];
+  double2 ab[KB];
+  double red[6][CfgSA<KB, RPT>::NW];
+};
+
+template <int KB, int RPT, bool ALL>
+__device__ __forceinline__ int solve_set_sa(const MatrixF32& M, const int* __restrict__ S, int k,
+                                             long long set, long long off, const SetOutputs& out,
+                                             SASmem<KB, RPT>& sm,
+                                             const Grp<CfgSA<KB, RPT>::NT>& g) {
+  using C = CfgSA<KB, RPT>;
+  constexpr int NT = C::NT;
+  constexpr int NW = C::NW;
+  constexpr int NCH = C::NCH;
+  const int t = g.t;
+
+  // ---- indices -> shared memory, validation ---------------------------------
+  bool bad = false;
+  for (int c = t; c < KB; c += NT) {
+    int v = 0;
+    if (c < k) {
+      v = __ldg(S + c);
+      bad |= (v < 0) | (v >= M.n);
+    }
+    sm.idx[c] = (c < k && v >= 0 && v < M.n) ? v : 0;
+  }
+  if (group_any<NT, NW>(bad, g, sm.red[3])) {
+    if (t == 0) write_failed(out, set, off, ALL ? k : 0, SET_BAD_INDEX);
+    g.sync();
+    return -1;
+  }
+  g.sync();
+
+  // ---- gather this thread's rows of A[S,S] into shared memory; P = I ----------
+  float4* __restrict__ my = sm.A + t;  // chunk (q, ch) at my[(q * NCH + ch) * NT]
+  float2 Pr[RPT][KB / 2];  // column pairs: packed FP32 (FFMA2) halves the FMA issues
+  double fro = 0.0;
+#pragma unroll
+  for (int q = 0; q < RPT; ++q) {
+    const int r = t + q * NT;
+    const bool rv = r < k;
+    const float* __restrict__ arow = M.A + (size_t)sm.idx[r] * (size_t)M.lda;
+#pragma unroll
+    for (int ch = 0; ch < NCH; ++ch) {
+      float e[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int c = 4 * ch + u;
+        e[u] = (rv && c < k) ? __ldg(arow + sm.idx[c]) : 0.f;
+        fro += (double)e[u] * (double)e[u];
+      }
+      Pr[q][2 * ch] = make_float2((rv && 4 * ch == r) ? 1.f : 0.f, (rv && 4 * ch + 1 == r) ? 1.f : 0.f);
+      Pr[q][2 * ch + 1] =
+          make_float2((rv && 4 * ch + 2 == r) ? 1.f : 0.f, (rv && 4 * ch + 3 == r) ? 1.f : 0.f);
+      my[(q * NCH + ch) * NT] = make_float4(e[0], e[1], e[2], e[3]);
+    }
+  }
+  const double fro2 = group_sum<NT, NW>(fro, g, sm.red[2]);
+  const double tau = 32.0 * (double)kEps32 * sqrt(fro2);
+
+  // ---- Lanczos with projector reorthogonalisation ----------------------------
+  float v[RPT], vp[RPT];
+  const float v0 = (float)(1.0 / sqrt((double)k));
+#pragma unroll
+  for (int q = 0; q < RPT; ++q) {
+    v[q] = (t + q * NT) < k ? v0 : 0.f;
+    vp[q] = 0.f;
+  }
+  for (int c = t; c < KB; c += NT) sm.vb[c] = c < k ? v0 : 0.f;
+  if (t == 0) sm.ab[0].y = 0.0;
+  float sc = 1.f, bprev = 0.f;
+  int status = 0;
+  g.sync();
+
+  for (int j = 0; j < k; ++j) {
+    // P -= v v^T and y = A v, one pass over the broadcast vector
+    float2 ya[RPT], yb[RPT], ncoef[RPT];
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      const float cq = -v[q] * sc;
+      ncoef[q] = make_float2(cq, cq);
+      ya[q] = make_float2(0.f, 0.f);
+      yb[q] = make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int ch = 0; ch < NCH; ++ch) {
+      const float4 b4 = *reinterpret_cast<const float4*>(&sm.vb[4 * ch]);
+      const float2 b01 = make_float2(b4.x, b4.y), b23 = make_float2(b4.z, b4.w);
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) {
+        const float4 a4 = my[(q * NCH + ch) * NT];
+        Pr[q][2 * ch] = __ffma2_rn(ncoef[q], b01, Pr[q][2 * ch]);
+        Pr[q][2 * ch + 1] = __ffma2_rn(ncoef[q], b23, Pr[q][2 * ch + 1]);
+        ya[q] = __ffma2_rn(make_float2(a4.x, a4.y), b01, ya[q]);
+        yb[q] = __ffma2_rn(make_float2(a4.z, a4.w), b23, yb[q]);
+      }
+    }
+    float yy[RPT];
+    double ap = 0.0;
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      yy[q] = ((ya[q].x + ya[q].y) + (yb[q].x + yb[q].y)) * sc;
+      ap = fma((double)v[q], (double)yy[q], ap);
+    }
+    const double alpha = group_sum<NT, NW>(ap, g, sm.red[0]);
+    const float af = (float)alpha;
+
+    float wt[RPT];
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      wt[q] = fmaf(-af, v[q], fmaf(-bprev, vp[q], yy[q]));
+      sm.wb[t + q * NT] = wt[q];
+    }
+    g.sync();
+
+    // w = P w~
+    float2 wa[RPT], wc[RPT];
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      wa[q] = make_float2(0.f, 0.f);
+      wc[q] = make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int ch = 0; ch < NCH; ++ch) {
+      const float4 x4 = *reinterpret_cast<const float4*>(&sm.wb[4 * ch]);
+      const float2 x01 = make_float2(x4.x, x4.y), x23 = make_float2(x4.z, x4.w);
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) {
+        wa[q] = __ffma2_rn(Pr[q][2 * ch], x01, wa[q]);
+        wc[q] = __ffma2_rn(Pr[q][2 * ch + 1], x23, wc[q]);
+      }
+    }
+    float ww[RPT];
+    double bp = 0.0;
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      ww[q] = (wa[q].x + wa[q].y) + (wc[q].x + wc[q].y);
+      bp = fma((double)ww[q], (double)ww[q], bp);
+      sm.vb[t + q * NT] = ww[q];  // published by the sync below
+    }
+    const double b2v = group_sum<NT, NW>(bp, g, sm.red[1]);
+    if constexpr (NW == 1) g.sync();
+    if (t == 0) {
+      sm.ab[j].x = alpha;
+      if (j + 1 < k) sm.ab[j + 1].y = b2v;
+    }
+    if (!isfinite(alpha) || !isfinite(b2v)) {
+      status |= SET_NONFINITE;
+      break;
+    }
+    if (j + 1 == k) break;
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) vp[q] = v[q];
+    if (b2v > tau * tau) {
+      const float bf = sqrtf((float)b2v);
+      const float inv = 1.0f / bf;
+      sc = inv;
+      bprev = bf;
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) v[q] = ww[q] * inv;
+    } else {
+      // Breakdown: restart with the column of P (orthogonal to every v so
+      // far) of largest diagonal; beta_{j+1} = 0 (decoupled block).
+      status |= SET_BREAKDOWN;
+      unsigned long long key = 0ull;
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) {
+        const int r = t + q * NT;
+        if (r < k) {
+          float d = 0.f;
+#pragma unroll
+          for (int c = 0; c < KB; c += 2) {
+            if (c == r) d = Pr[q][c / 2].x;
+            if (c + 1 == r) d = Pr[q][c / 2].y;
+          }
+          d = fmaxf(d, 0.f);
+          const unsigned long long kk =
+              ((unsigned long long)__float_as_uint(d) << 32) | (unsigned)(0x7fffffff - r);
+          key = kk > key ? kk : key;
+        }
+      }
+      key = group_max_u64<NT, NW>(key, g, sm.red[3]);
+      const int m = 0x7fffffff - (int)(key & 0xffffffffu);
+      g.sync();
+#pragma unroll
+      for (int q = 0; q < RPT; ++q)
+        if (t + q * NT == m) {
+#pragma unroll
+          for (int c = 0; c < KB; c += 2) {
+            sm.vb[c] = Pr[q][c / 2].x;
+            sm.vb[c + 1] = Pr[q][c / 2].y;
+          }
+        }
+      g.sync();
+      double zp = 0.0;
+      float z[RPT];
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) {
+        z[q] = sm.vb[t + q * NT];
+        zp += (double)z[q] * (double)z[q];
+      }
+      const double zz = group_sum<NT, NW>(zp, g, sm.red[1]);
+      if (t == 0) sm.ab[j + 1].y = 0x1p-600;  // decoupled block (see sturm_count)
+      const float inv = 1.0f / sqrtf((float)zz);
+      sc = inv;
+      bprev = 0.f;
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) v[q] = z[q] * inv;
+    }
+  }
+  g.sync();  // T visible to every thread
+
+  if constexpr (!ALL) {
+    // extremes mode: T stays in sm.ab for the caller's deferred bisection
+    return status;
+  }
+  if (status & SET_NONFINITE) {
+    if (t == 0) write_failed(out, set, off, ALL ? k : 0, status);
+    g.sync();
+    return -1;
+  }
+
+  // ---- eigenvalues of T by FP64 Sturm bisection --------------------------------
+  double glo = 1e300, ghi = -1e300;
+  for (int i = t; i < k; i += NT) {
+    const double rad = (i > 0 ? sqrt(sm.ab[i].y) : 0.0) + (i + 1 < k ? sqrt(sm.ab[i + 1].y) : 0.0);
+    glo = fmin(glo, sm.ab[i].x - rad);
+    ghi = fmax(ghi, sm.ab[i].x + rad);
+  }
+  glo = group_minmax<NT, NW, false>(glo, g, sm.red[2]);
+  ghi = group_minmax<NT, NW, true>(ghi, g, sm.red[3]);
+  {
+    const double pad = 0x1p-51 * fmax(fabs(glo), fabs(ghi)) + 1e-300;
+    glo -= pad;
+    ghi += pad;
+  }
+  {
+    int R = 0;
+    {
+      double wdt = ghi - glo, tol = bisect_tol(glo, ghi);
+      while (wdt > tol && R < 200) {
+        wdt *= 0.5;
+        ++R;
+      }
+    }
+    double prod = 1.0;
+    for (int m = t; m < k; m += NT) {
+      const double e = bisect_index(sm.ab, k, m, glo, ghi, R);
+      if (out.eig) out.eig[off + m] = e;
+      prod *= e;
+      if (m == 0) {
+        sm.red[4][0] = e;
+        if (out.lmin) out.lmin[set] = e;
+      }
+      if (m == k - 1) {
+        sm.red[5][0] = e;
+        if (out.lmax) out.lmax[set] = e;
+      }
+    }
+    constexpr int W = NT < 32 ? NT : 32;
+#pragma unroll
+    for (int o = W / 2; o > 0; o >>= 1) prod *= __shfl_xor_sync(g.mask, prod, o);
+    if constexpr (NW > 1) {
+      if ((threadIdx.x & 31) == 0) sm.red[0][g.wig] = prod;
+    }
+    g.sync();
+    if (t == 0) {
+      double det = prod;
+      if constexpr (NW > 1) {
+        det = sm.red[0][0];
+        for (int w2 = 1; w2 < NW; ++w2) det *= sm.red[0][w2];
+      }
+      if (out.det) out.det[set] = det;
+      if (out.delta) out.delta[set] = fmax(1.0 - sm.red[4][0], sm.red[5][0] - 1.0);
+      if (out.err) out.err[set] = status;
+    }
+  }
+  g.sync();
+  return -1;
+}
+
+}  // namespace pl

@@ -3,7 +3,9 @@
 #pragma once
 #include "pl_cgs.cuh"
 #include "pl_engine.cuh"
+#include "pl_engine_sa.cuh"
 #include "pl_indexgen.cuh"
+#include "pl_queue.cuh"
 
 namespace pl {
 
@@ -13,17 +15,21 @@ namespace pl {
 // ---------------------------------------------------------------------------
 template <int KB, int RPT, int TPR, int CTA, int MINB, bool ALL>
 __global__ void __launch_bounds__(CTA, MINB)
-    k_reg_solve(MatrixF32 M, SetSource src, SetOutputs out) {
+    k_reg_solve(MatrixF32 M, SetSource src, SetOutputs out, double2* __restrict__ qbuf) {
   using C = Cfg<KB, RPT, TPR>;
   constexpr int GPC = CTA / C::NT;
+  constexpr int Q = C::NT / 2;
   static_assert(CTA % C::NT == 0, "CTA must hold whole groups");
   static_assert(C::NT <= 32 || GPC <= 15, "named barrier ids");
   __shared__ GroupSmem<KB, C::NW> smem[GPC];
+  __shared__ QueueMeta qmeta[GPC][Q];
   const Grp<C::NT> g = make_group<C::NT>();
   const int gic = threadIdx.x / C::NT;
   const long long ng = (long long)gridDim.x * GPC;
   const long long nitems = item_count(src);
   const int pbase = src.perm_start ? *src.perm_start : 0;
+  double2* __restrict__ T = qbuf + ((size_t)blockIdx.x * GPC + gic) * (size_t)(Q * KB);
+  int nq = 0;
   for (long long it = (long long)blockIdx.x * GPC + gic; it < nitems; it += ng) {
     long long set, off;
     int k;
@@ -32,7 +38,85 @@ __global__ void __launch_bounds__(CTA, MINB)
       if (g.t == 0) write_failed(out, set, off, 0, SET_BAD_K);
       continue;
     }
-    solve_set<KB, RPT, TPR, ALL>(M, src.idx + off, k, set, off, out, smem[gic], g);
+    // the slot's metadata goes to shared memory first, so the set id and k
+    // need no registers across the Lanczos loop
+    if constexpr (!ALL) {
+      if (g.t == 0) qmeta[gic][nq] = QueueMeta{set, k, 0};
+    }
+    const int st = solve_set<KB, RPT, TPR, ALL>(M, src.idx + off, k, set, off, out, smem[gic], g);
+    if constexpr (!ALL) {
+      if (st >= 0) {
+        const int kq = qmeta[gic][nq].k;
+        for (int i = g.t; i < kq; i += C::NT) T[(size_t)i * Q + nq] = smem[gic].ab[i];
+        if (g.t == 0) qmeta[gic][nq].status = st;
+        ++nq;
+        g.sync();
+        if (nq == Q) {
+          queue_bisect(T, Q, nq, qmeta[gic], g.t, out, g.mask);
+          g.sync();
+          nq = 0;
+        }
+      }
+    }
+  }
+  if constexpr (!ALL) {
+    if (nq > 0) queue_bisect(T, Q, nq, qmeta[gic], g.t, out, g.mask);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Batched form, shared-A engine (pl_engine_sa.cuh): persistent, A_S in
+// dynamic shared memory, P in registers.
+// ---------------------------------------------------------------------------
+template <int KB, int RPT, int CTA, int MINB, bool ALL>
+__global__ void __launch_bounds__(CTA, MINB)
+    k_sa_solve(MatrixF32 M, SetSource src, SetOutputs out, double2* __restrict__ qbuf) {
+  using C = CfgSA<KB, RPT>;
+  constexpr int GPC = CTA / C::NT;
+  constexpr int Q = C::NT / 2;
+  static_assert(CTA % C::NT == 0, "CTA must hold whole groups");
+  static_assert(C::NT <= 32 || GPC <= 15, "named barrier ids");
+  extern __shared__ __align__(16) float dsm[];
+  SASmem<KB, RPT>* smem = reinterpret_cast<SASmem<KB, RPT>*>(dsm);
+  __shared__ QueueMeta qmeta[GPC][Q];
+  const Grp<C::NT> g = make_group<C::NT>();
+  const int gic = threadIdx.x / C::NT;
+  const long long ng = (long long)gridDim.x * GPC;
+  const long long nitems = item_count(src);
+  const int pbase = src.perm_start ? *src.perm_start : 0;
+  double2* __restrict__ T = qbuf + ((size_t)blockIdx.x * GPC + gic) * (size_t)(Q * KB);
+  int nq = 0;
+  for (long long it = (long long)blockIdx.x * GPC + gic; it < nitems; it += ng) {
+    long long set, off;
+    int k;
+    set_span(src, it, pbase, set, off, k);
+    if (k < 1 || k > KB) {
+      if (g.t == 0) write_failed(out, set, off, 0, SET_BAD_K);
+      continue;
+    }
+    // the slot's metadata goes to shared memory first, so the set id and k
+    // need no registers across the Lanczos loop
+    if constexpr (!ALL) {
+      if (g.t == 0) qmeta[gic][nq] = QueueMeta{set, k, 0};
+    }
+    const int st = solve_set_sa<KB, RPT, ALL>(M, src.idx + off, k, set, off, out, smem[gic], g);
+    if constexpr (!ALL) {
+      if (st >= 0) {
+        const int kq = qmeta[gic][nq].k;
+        for (int i = g.t; i < kq; i += C::NT) T[(size_t)i * Q + nq] = smem[gic].ab[i];
+        if (g.t == 0) qmeta[gic][nq].status = st;
+        ++nq;
+        g.sync();
+        if (nq == Q) {
+          queue_bisect(T, Q, nq, qmeta[gic], g.t, out, g.mask);
+          g.sync();
+          nq = 0;
+        }
+      }
+    }
+  }
+  if constexpr (!ALL) {
+    if (nq > 0) queue_bisect(T, Q, nq, qmeta[gic], g.t, out, g.mask);
   }
 }
 

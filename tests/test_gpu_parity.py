@@ -21,6 +21,12 @@ GOLD = os.path.join(os.path.dirname(__file__), "golden")
 RTOL = 1e-5
 
 
+def ok(err):
+    """No error bits; PL_SET_BREAKDOWN is informational (the recurrence was
+    restarted and the result is valid)."""
+    return ((np.asarray(err) & ~_lib.PL_SET_BREAKDOWN) == 0).all()
+
+
 def _torch():
     import torch
     return torch
@@ -78,7 +84,7 @@ def test_uniform_k_vs_oracle_and_dsyev(k, form):
     nsets = 96 if k <= 64 else 24
     o, idx = O.gen_stream(1, 0, nsets, A.shape[0], 0, k, k)
     res = run(A, idx, k=k, form=form)
-    assert (res["err"] == 0).all()
+    assert ok(res["err"])
     orc = O.batch(A, idx, k=k)
     np.testing.assert_array_less(np.abs(res["lmin"] - orc["lmin"]), RTOL * np.abs(orc["lmin"]))
     np.testing.assert_array_less(np.abs(res["lmax"] - orc["lmax"]), RTOL * np.abs(orc["lmax"]))
@@ -91,7 +97,7 @@ def test_all_eigenvalues_vs_dsyev(k):
     nsets = 32 if k <= 64 else 8
     o, idx = O.gen_stream(2, 0, nsets, A.shape[0], 0, k, k)
     res = run(A, idx, k=k, want_all=True)
-    assert (res["err"] == 0).all()
+    assert ok(res["err"])
     check_vs_dsyev(A, idx, k, res)
 
 
@@ -101,7 +107,7 @@ def test_large_k_vs_dsyev(k):
     nsets = 4
     o, idx = O.gen_stream(3, 0, nsets, A.shape[0], 0, k, k)
     res = run(A, idx, k=k)
-    assert (res["err"] == 0).all()
+    assert ok(res["err"])
     check_vs_dsyev(A, idx, k, res, all_k=False)
 
 
@@ -109,7 +115,7 @@ def test_uneven_k_csr_vs_dsyev():
     A = cached_gram(1024, 4096)
     offs, idx = O.gen_stream(5, 0, 600, 4096, 1, 8, 256)
     res = run(A, idx, offsets=offs)
-    assert (res["err"] == 0).all()
+    assert ok(res["err"])
     check_vs_dsyev(A, idx, None, res, offsets=offs, all_k=False)
     # the captured graph is reused on the second call: same results, bitwise
     res2 = run(A, idx, offsets=offs)
@@ -122,7 +128,7 @@ def test_uneven_k_plain_form_and_all():
     offs, idx = O.gen_stream(6, 0, 200, 2048, 2, 2, 140)
     for form in ("plain", "batched"):
         res = run(A, idx, offsets=offs, form=form, want_all=True)
-        assert (res["err"] == 0).all()
+        assert ok(res["err"])
         check_vs_dsyev(A, idx, None, res, offsets=offs)
 
 
@@ -206,13 +212,13 @@ def test_bad_indices_and_k_reported_per_set():
     A = cached_gram(256, 512)
     idx = np.array([0, 1, 2, 3, 5, -1, 7, 8, 9, 10, 11, 512], np.int32)
     res = run(A, idx, k=4)
-    assert res["err"][0] == 0
+    assert ok(res["err"][:1])
     assert res["err"][1] & _lib.PL_SET_BAD_INDEX and np.isnan(res["lmin"][1])
     assert res["err"][2] & _lib.PL_SET_BAD_INDEX and np.isnan(res["lmax"][2])
     offs = np.array([0, 4, 4 + 600], np.int64)
     idx2 = np.r_[np.arange(4), np.arange(600) % 512].astype(np.int32)
     res = run(cached_gram(256, 1024), idx2, offsets=offs)
-    assert res["err"][0] == 0 and res["err"][1] & _lib.PL_SET_BAD_K
+    assert ok(res["err"][:1]) and res["err"][1] & _lib.PL_SET_BAD_K
 
 
 def test_nonfinite_input():
