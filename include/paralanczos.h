@@ -81,6 +81,19 @@ int pl_solve(const float *A, int n, long long lda, const int *idx, const long lo
              long long nsets, int k, int form, double *lmin, double *lmax, double *delta,
              int *err, double *eig, double *det, void *stream);
 
+/* Allocation-free variant of pl_solve for callers that cannot call cudaMalloc
+ * (a host runtime that owns the device-memory budget, code running during a
+ * CUDA graph capture, plugins that must not allocate after start-up).  No
+ * counterpart in the reference.  Uniform k only, 1 <= k <= 64, extremes only
+ * (lambda_min, lambda_max, delta_k, err); device pointers, asynchronous on
+ * `stream`.  The kernels' scratch lives in a static 32 MiB device array of the
+ * library (held by every GPU that loads it until exit) instead of cudaMalloc'd
+ * memory; k > 64 returns PL_ENOTSUP.  The first call on a device looks up the
+ * array's device address, so make that first call before any stream capture.
+ * All calls share the array: calls whose kernels overlap on the GPU race.    */
+int pl_solve_noalloc(const float *A, int n, long long lda, const int *idx, long long nsets, int k,
+                     double *lmin, double *lmax, double *delta, int *err, void *stream);
+
 /* Same with HOST buffers: copies A and the sets in, solves, copies results out
  * (synchronous).  offsets/eig/det/lmin/lmax/delta/err nullable as above.     */
 int pl_solve_host(const float *A, int n, long long lda, const int *idx, const long long *offsets,

@@ -28,6 +28,7 @@ SIGNATURES = {
     "pl_last_cuda_error": (_i, []),
     "pl_solve": (_i, [_vp, _i, _ll, _vp, _vp, _ll, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "pl_solve_host": (_i, [_vp, _i, _ll, _vp, _vp, _ll, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "pl_solve_noalloc": (_i, [_vp, _i, _ll, _vp, _ll, _i, _vp, _vp, _vp, _vp, _vp]),
     "pl_gen_sets": (_i, [C.c_ulonglong, _ll, _ll, _i, _i, _vp, _vp]),
     "pl_gen_stream_host": (_ll, [C.c_ulonglong, _ll, _ll, _i, _i, _i, _i, _vp, _vp]),
     "pl_convert_f64_f32": (_i, [_vp, _vp, _ll, _vp]),

@@ -454,6 +454,41 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 }  // namespace
 
 // =============================================================================
+// Allocation-free entry point (pl_solve_noalloc)
+// =============================================================================
+// Some callers cannot call cudaMalloc: a host that owns the device memory
+// budget (an embedding runtime or a serving process that pre-partitions HBM),
+// code running while a CUDA graph is being captured, or a plugin whose
+// contract forbids allocation after start-up.  For them the batched k <= 64
+// kernels can run with their deferred-bisection queues in this file-scope
+// array instead of a cudaMalloc'd buffer.  32 MiB covers the full persistent
+// grid of every k <= 64 kernel; every GPU that loads the library holds the
+// array until the process exits.  All calls share it and it keeps the last
+// call's contents (nothing in it has to start at zero: a queue slot is written
+// before it is read), so calls whose kernels overlap on the GPU race.
+constexpr size_t kNoAllocBytes = size_t(32) << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+namespace {
+void* g_noalloc_ptr[64] = {};
+
+// Once per device, with that device current: the array's device address (the
+// symbol itself is only a host-side stand-in).
+int noalloc_setup(void** out) {
+  int dev = 0;
+  PL_CU(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return PL_ENOTSUP;
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    PL_CU(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return PL_OK;
+}
+}  // namespace
+
+// =============================================================================
 // C ABI
 // =============================================================================
 extern "C" {
@@ -481,6 +516,25 @@ int pl_solve(const float* A, int n, long long lda, const int* idx, const long lo
   std::lock_guard<std::mutex> lk(g_mu);
   SetOutputs out{lmin, lmax, delta, err, eig, det};
   return solve_dev(A, n, lda, idx, offsets, nsets, k, form, out, (cudaStream_t)stream);
+}
+
+int pl_solve_noalloc(const float* A, int n, long long lda, const int* idx, long long nsets, int k,
+                     double* lmin, double* lmax, double* delta, int* err, void* stream) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  int rc = validate_common(A, n, lda, idx, nsets, k, nullptr, PL_FORM_BATCHED);
+  if (rc || nsets == 0) return rc;
+  const int b = bin_of_k(k);
+  if (b < 0 || kBinK[b] > 64) return PL_ENOTSUP;  // only the k <= 64 kernels fit the array
+  const Variant& v = chosen(b);
+  if (v.scratch[0]() > kNoAllocBytes) return PL_ENOTSUP;
+  void* scratch = nullptr;
+  rc = noalloc_setup(&scratch);
+  if (rc) return rc;
+  MatrixF32 M{A, lda, n};
+  SetSource src{idx, nullptr, k, nullptr, nullptr, nullptr, nsets};
+  SetOutputs out{lmin, lmax, delta, err, nullptr, nullptr};
+  PL_CU(v.fn[0](M, src, out, nsets, scratch, (cudaStream_t)stream, false));
+  return PL_OK;
 }
 
 int pl_solve_host(const float* A, int n, long long lda, const int* idx, const long long* offsets,
