@@ -47,6 +47,15 @@ int device_sms() {
 
 // nitems < 0: the item count lives on the device.  prep: only load the kernel
 // and cache its launch attributes (done before a stream capture starts).
+// PL_VERBOSE=2 logs launch configurations to stderr.
+int verbosity() {
+  static int v = [] {
+    const char* e = getenv("PL_VERBOSE");
+    return e ? atoi(e) : 0;
+  }();
+  return v;
+}
+
 typedef cudaError_t (*LaunchFn)(const MatrixF32&, const SetSource&, const SetOutputs&, long long,
                                 void*, cudaStream_t, bool prep);
 // Bytes of device scratch a variant needs at its full (persistent) grid.
@@ -159,6 +168,38 @@ cudaError_t launch_large(const MatrixF32& M, const SetSource& src, const SetOutp
   return cudaGetLastError();
 }
 
+template <int KB, int CS, int NTC>
+cudaError_t launch_cluster(const MatrixF32& M, const SetSource& src, const SetOutputs& out,
+                           long long nitems, void*, cudaStream_t st, bool prep) {
+  auto kern = k_cluster_solve<KB, CS, NTC>;
+  const size_t dsm = sizeof(ClusterSmem<KB, CS, NTC>);
+  static int maxcl = [&] {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
+    cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(CS * 64, 1, 1);
+    cfg.blockDim = dim3(NTC, 1, 1);
+    cfg.dynamicSmemBytes = dsm;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess || n < 1) {
+      cudaGetLastError();
+      n = device_sms() / CS;
+    }
+    return n;
+  }();
+  if (prep) {
+    cudaFuncAttributes fa;
+    return cudaFuncGetAttributes(&fa, kern);
+  }
+  long long ncl = maxcl;
+  if (nitems >= 0 && nitems < ncl) ncl = nitems > 0 ? nitems : 1;
+  if (verbosity() >= 2)
+    fprintf(stderr, "paralanczos: cluster KB=%d CS=%d NTC=%d: %lld clusters (max resident %d), %zu B smem/CTA\n",
+            KB, CS, NTC, ncl, maxcl, dsm);
+  kern<<<(unsigned)(ncl * CS), NTC, dsm, st>>>(M, src, out);
+  return cudaGetLastError();
+}
+
 template <int KM>
 size_t scratch_large() {
   return sizeof(float) * 2 * (size_t)KM * KM * (size_t)device_sms();
@@ -183,14 +224,19 @@ struct Variant {
         {launch_sa<KB, RPT, CTA, MINB, false>, launch_sa<KB, RPT, CTA, MINB, true>},          \
         {scratch_sa<KB, RPT, CTA, MINB, false>, scratch_none}                                  \
   }
+#define CLUSTER(KB, CS, NTC)                                                                  \
+  Variant {                                                                                     \
+    "cluster KB=" #KB " CS=" #CS " NTC=" #NTC,                                                  \
+        {launch_cluster<KB, CS, NTC>, nullptr}, {scratch_none, scratch_none}                    \
+  }
 #define LARGE(KM) \
   Variant {                                                                             \
     "large KM=" #KM " CTA=256", {launch_large<KM, false>, launch_large<KM, true>},      \
         {scratch_large<KM>, scratch_large<KM>}                                           \
   }
 
-const int kBinK[] = {8, 16, 32, 64, 128, 256, 512};
-constexpr int kNumBins = 7;
+const int kBinK[] = {8, 16, 32, 64, 128, 192, 256, 384, 512};
+constexpr int kNumBins = 9;
 
 const std::vector<Variant>& variants(int b) {
   static const std::vector<Variant> v[kNumBins] = {
@@ -199,13 +245,15 @@ const std::vector<Variant>& variants(int b) {
       {REG(32, 2, 1, 128, 3), REG(32, 1, 1, 128, 4), SA(32, 2, 128, 4)},
       {REG(64, 1, 1, 128, 3), SA(64, 2, 128, 3), REG(64, 1, 1, 128, 2), SA(64, 2, 128, 2)},
       {SA(128, 1, 128, 3), REG(128, 1, 2, 256, 1), SA(128, 1, 128, 2)},
-      {LARGE(256)},
-      {LARGE(512)},
+      {CLUSTER(192, 2, 384), LARGE(256), CLUSTER(192, 4, 192)},
+      {CLUSTER(256, 2, 512), LARGE(256), CLUSTER(256, 4, 256), CLUSTER(256, 8, 256)},
+      {CLUSTER(384, 4, 384), LARGE(512), CLUSTER(384, 8, 192)},
+      {CLUSTER(512, 8, 256), LARGE(512), CLUSTER(512, 8, 512)},
   };
   return v[b];
 }
 
-int g_variant[kNumBins] = {0, 0, 0, 0, 0, 0, 0};
+int g_variant[kNumBins] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 
 int bin_of_k(int k) {
   for (int b = 0; b < kNumBins; ++b)
@@ -218,6 +266,16 @@ const Variant& chosen(int b) {
   int i = g_variant[b];
   if (i < 0 || i >= (int)v.size()) i = 0;
   return v[i];
+}
+
+// The chosen variant if it implements the requested mode (extremes / all
+// eigenvalues), else the first variant of the bin that does.
+const Variant& chosen_for(int b, bool all) {
+  const Variant& v = chosen(b);
+  if (v.fn[all ? 1 : 0]) return v;
+  for (const Variant& w : variants(b))
+    if (w.fn[all ? 1 : 0]) return w;
+  return v;
 }
 
 // Plain form kernels by k bin (k <= 128).
@@ -309,7 +367,7 @@ int solve_uniform(const MatrixF32& M, const int* idx, long long nsets, int k, in
   }
   const int b = bin_of_k(k);
   if (b < 0) return PL_ENOTSUP;
-  const Variant& v = chosen(b);
+  const Variant& v = chosen_for(b, all);
   void* scratch = nullptr;
   const size_t need = v.scratch[all ? 1 : 0]();
   if (need) {
@@ -340,7 +398,7 @@ int solve_csr(const MatrixF32& M, const int* idx, const long long* offsets, long
   for (int b = 0; b < nb; ++b) {
     large_off[b] = large_total;
     const bool plain_bin = form == PL_FORM_PLAIN && kBinK[b] <= 128;
-    const size_t need = plain_bin ? 0 : chosen(b).scratch[all ? 1 : 0]();
+    const size_t need = plain_bin ? 0 : chosen_for(b, all).scratch[all ? 1 : 0]();
     large_total += (need + 255) & ~(size_t)255;
   }
   rc = ensure(d.large, large_total > 0 ? large_total : 256);
@@ -350,7 +408,7 @@ int solve_csr(const MatrixF32& M, const int* idx, const long long* offsets, long
            (const void*)M.A, M.n, M.lda, (const void*)idx, (const void*)offsets, nsets, form,
            (void*)out.lmin, (void*)out.lmax, (void*)out.delta, (void*)out.err, (void*)out.eig,
            (void*)out.det, g_variant[0], g_variant[1], g_variant[2], g_variant[3], g_variant[4],
-           g_variant[5], g_variant[6]);
+           g_variant[5], g_variant[6], g_variant[7] * 10 + g_variant[8]);
   const std::string key(keybuf);
   auto it = d.graphs.find(key);
   if (it == d.graphs.end()) {
@@ -364,7 +422,7 @@ int solve_csr(const MatrixF32& M, const int* idx, const long long* offsets, long
     LaunchFn fns[kNumBins];
     for (int b = 0; b < nb; ++b) {
       fns[b] = (form == PL_FORM_PLAIN && kBinK[b] <= 128) ? plain_fn(kBinK[b], all)
-                                                          : chosen(b).fn[all ? 1 : 0];
+                                                          : chosen_for(b, all).fn[all ? 1 : 0];
       // load every kernel before the capture: nothing that may load a module
       // or set a function attribute runs while the stream is capturing
       PL_CU(fns[b](M, SetSource{}, out, 0, nullptr, d.side[b], true));

@@ -1,0 +1,307 @@
+// pl_cluster.cuh -- large-k per-set Lanczos on a thread-block cluster.
+//
+// For 128 < k <= 512 the per-set state (A_S and the projector P, 2 k^2 floats:
+// 512 KB at k = 256, 2 MB at k = 512) does not fit one SM.  A cluster of CS
+// CTAs (one per SM) holds one set: CTA c owns rows [c R, c R + R), R = KB/CS,
+// with its rows of A_S in shared memory (lane-interleaved float4 layout) and
+// its rows of P in registers.  Same recurrence as pl_engine.cuh (three-term
+// step, w = P w~, P -= v v^T fused with the next matvec, FP32 vectors, FP64
+// alpha/beta).  Per step the CTAs exchange, through distributed shared memory:
+// their FP64 partials of alpha and ||w||^2 (every CTA sums the CS partials in
+// rank order, so the scalars are bitwise identical cluster-wide and every
+// branch is cluster-uniform), and their rows of w~ and w (written into every
+// peer's broadcast buffers).  Two cluster barriers per step: one carries the
+// rows of y = A v with the alpha partials (each CTA then forms all of
+// w~ = y - alpha v_j - beta_j v_{j-1} locally), one carries the rows of w with
+// the ||w||^2 partials.
+//
+// Thread mapping inside a CTA: NTC threads, TPR = NTC / R threads per row, a
+// thread owns CPT = KB / TPR consecutive columns of its row; row partial sums
+// are combined with xor-shuffles over the TPR lanes (TPR divides 32).
+#pragma once
+#include <cooperative_groups.h>
+
+#include "pl_engine.cuh"
+#include "pl_sturm.cuh"
+
+namespace pl {
+
+namespace cg = cooperative_groups;
+
+template <int KB, int CS, int NTC>
+struct CfgC {
+  static constexpr int R = KB / CS;       // rows per CTA
+  static constexpr int TPR = NTC / R;     // threads per row
+  static constexpr int CPT = KB / TPR;    // columns per thread
+  static constexpr int NCH = CPT / 4;     // float4 chunks per thread
+  static constexpr int NWC = NTC / 32;    // warps per CTA
+  static_assert(KB % CS == 0 && NTC % R == 0 && KB % TPR == 0, "bad shape");
+  static_assert(32 % TPR == 0 && CPT % 4 == 0, "bad shape");
+};
+
+template <int KB, int CS, int NTC>
+struct __align__(16) ClusterSmem {
+  float4 A[(KB / CS) * KB / 4];  // own rows, [chunk][thread]
+  float vb[3][KB];               // unnormalised Lanczos vectors, rotating: current, previous, next
+  float yb[KB];                  // broadcast of y = A v
+  float wb[KB];                  // w~, formed locally from yb
+  int idx[KB];
+  double2 ab[KB];                // T (rank 0 reads it for the bisection)
+  double part[4][CS];            // partials from every rank: alpha, ||w||^2, misc, index check
+  double red[NTC / 32];          // warp partials inside the CTA
+  unsigned long long key[CS];    // breakdown argmax exchange
+};
+
+// Sum over the CTA, then over the cluster (rank order).  Identical everywhere.
+template <int KB, int CS, int NTC>
+__device__ __forceinline__ double cluster_sum(double x, ClusterSmem<KB, CS, NTC>& sm, int slot,
+                                              cg::cluster_group& cl, int rank) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) sm.red[w] = x;
+  __syncthreads();
+  if (threadIdx.x < CS) {
+    double s = sm.red[0];
+#pragma unroll
+    for (int i = 1; i < NTC / 32; ++i) s += sm.red[i];
+    ClusterSmem<KB, CS, NTC>* peer = cl.map_shared_rank(&sm, (unsigned)threadIdx.x);
+    peer->part[slot][rank] = s;
+  }
+  cl.sync();
+  double s = sm.part[slot][0];
+#pragma unroll
+  for (int r = 1; r < CS; ++r) s += sm.part[slot][r];
+  return s;
+}
+
+template <int KB, int CS, int NTC>
+__device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int* __restrict__ S,
+                                                  int k, long long set, const SetOutputs& out,
+                                                  ClusterSmem<KB, CS, NTC>& sm,
+                                                  cg::cluster_group& cl, int rank) {
+  using C = CfgC<KB, CS, NTC>;
+  constexpr int R = C::R, TPR = C::TPR, CPT = C::CPT, NCH = C::NCH;
+  const int t = threadIdx.x;
+  const int lr = t / TPR;              // local row
+  const int r = rank * R + lr;         // global row
+  const int c0 = (t % TPR) * CPT;      // first owned column
+  const bool lead = (t % TPR) == 0;
+  const unsigned rmask = (TPR == 32) ? 0xffffffffu : (((1u << TPR) - 1u) << ((t & 31) / TPR * TPR));
+
+  // ---- indices (every CTA keeps the full set), validation -------------------
+  bool bad = false;
+  for (int c = t; c < KB; c += NTC) {
+    int v = 0;
+    if (c < k) {
+      v = __ldg(S + c);
+      bad |= (v < 0) | (v >= M.n);
+    }
+    sm.idx[c] = (c < k && v >= 0 && v < M.n) ? v : 0;
+  }
+  const double badsum = cluster_sum<KB, CS, NTC>(__any_sync(0xffffffffu, bad) ? 1.0 : 0.0, sm, 3, cl, rank);
+  if (badsum != 0.0) {
+    if (rank == 0 && t == 0) write_failed(out, set, 0, 0, SET_BAD_INDEX);
+    cl.sync();
+    return;
+  }
+
+  // ---- gather own rows of A_S into shared memory; P = I ----------------------
+  float4* __restrict__ my = sm.A + t;  // chunk ch at my[ch * NTC]
+  float2 Pr[CPT / 2];
+  double fro = 0.0;
+  {
+    const bool rv = r < k;
+    const float* __restrict__ arow = M.A + (size_t)sm.idx[r] * (size_t)M.lda;
+#pragma unroll
+    for (int ch = 0; ch < NCH; ++ch) {
+      float e[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int c = c0 + 4 * ch + u;
+        e[u] = (rv && c < k) ? __ldg(arow + sm.idx[c]) : 0.f;
+        fro += (double)e[u] * (double)e[u];
+      }
+      my[ch * NTC] = make_float4(e[0], e[1], e[2], e[3]);
+      const int c = c0 + 4 * ch;
+      Pr[2 * ch] = make_float2((rv && c == r) ? 1.f : 0.f, (rv && c + 1 == r) ? 1.f : 0.f);
+      Pr[2 * ch + 1] = make_float2((rv && c + 2 == r) ? 1.f : 0.f, (rv && c + 3 == r) ? 1.f : 0.f);
+    }
+  }
+  const double fro2 = cluster_sum<KB, CS, NTC>(fro, sm, 2, cl, rank);
+  const double tau2 = (32.0 * (double)kEps32) * (32.0 * (double)kEps32) * fro2;
+
+  // vb[cur] holds the unnormalised v_j (v_j = sc * vb[cur]), vb[prv] v_{j-1}
+  // (scaled by scp); w is published into vb[nxt].  Peers write vb[nxt] and yb
+  // only after a cluster barrier that follows every read of the old contents.
+  const float v0 = (float)(1.0 / sqrt((double)k));
+  float v = r < k ? v0 : 0.f;
+  for (int c = t; c < KB; c += NTC) {
+    sm.vb[0][c] = c < k ? v0 : 0.f;
+    sm.vb[1][c] = 0.f;
+  }
+  if (t == 0) sm.ab[0].y = 0.0;
+  float sc = 1.f, scp = 0.f, bprev = 0.f;
+  int status = 0;
+  int cur = 0, prv = 1, nxt = 2;
+  __syncthreads();
+
+  for (int j = 0; j < k; ++j) {
+    // P -= v v^T and y = A v over the owned row slice
+    float2 ya = make_float2(0.f, 0.f), yb = make_float2(0.f, 0.f);
+    const float cq = -v * sc;
+    const float2 nc = make_float2(cq, cq);
+#pragma unroll
+    for (int ch = 0; ch < NCH; ++ch) {
+      const float4 b4 = *reinterpret_cast<const float4*>(&sm.vb[cur][c0 + 4 * ch]);
+      const float4 a4 = my[ch * NTC];
+      const float2 b01 = make_float2(b4.x, b4.y), b23 = make_float2(b4.z, b4.w);
+      Pr[2 * ch] = __ffma2_rn(nc, b01, Pr[2 * ch]);
+      Pr[2 * ch + 1] = __ffma2_rn(nc, b23, Pr[2 * ch + 1]);
+      ya = __ffma2_rn(make_float2(a4.x, a4.y), b01, ya);
+      yb = __ffma2_rn(make_float2(a4.z, a4.w), b23, yb);
+    }
+    float y = ((ya.x + ya.y) + (yb.x + yb.y)) * sc;
+#pragma unroll
+    for (int o = TPR / 2; o > 0; o >>= 1) y += __shfl_xor_sync(rmask, y, o);
+    // publish the owned rows of y with the alpha partial: one cluster barrier
+    if (lead) {
+#pragma unroll
+      for (int q = 0; q < CS; ++q) cl.map_shared_rank(&sm, (unsigned)q)->yb[r] = y;
+    }
+    const double alpha = cluster_sum<KB, CS, NTC>(lead ? (double)v * (double)y : 0.0, sm, 0, cl, rank);
+    const float af = (float)alpha;
+
+    // w~ = y - alpha v_j - beta_j v_{j-1}, every element formed locally
+    for (int c = t; c < KB; c += NTC)
+      sm.wb[c] = fmaf(-af, sc * sm.vb[cur][c], fmaf(-bprev, scp * sm.vb[prv][c], sm.yb[c]));
+    __syncthreads();
+
+    // w = P w~ over the owned row slice
+    float2 wa = make_float2(0.f, 0.f), wc = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int ch = 0; ch < NCH; ++ch) {
+      const float4 x4 = *reinterpret_cast<const float4*>(&sm.wb[c0 + 4 * ch]);
+      wa = __ffma2_rn(Pr[2 * ch], make_float2(x4.x, x4.y), wa);
+      wc = __ffma2_rn(Pr[2 * ch + 1], make_float2(x4.z, x4.w), wc);
+    }
+    float w = (wa.x + wa.y) + (wc.x + wc.y);
+#pragma unroll
+    for (int o = TPR / 2; o > 0; o >>= 1) w += __shfl_xor_sync(rmask, w, o);
+    if (lead) {
+#pragma unroll
+      for (int q = 0; q < CS; ++q) cl.map_shared_rank(&sm, (unsigned)q)->vb[nxt][r] = w;
+    }
+    const double b2v = cluster_sum<KB, CS, NTC>(lead ? (double)w * (double)w : 0.0, sm, 1, cl, rank);
+    if (t == 0 && rank == 0) {
+      sm.ab[j].x = alpha;
+      if (j + 1 < k) sm.ab[j + 1].y = b2v;
+    }
+    if (!isfinite(alpha) || !isfinite(b2v)) {
+      status |= SET_NONFINITE;
+      break;
+    }
+    if (j + 1 == k) break;
+    if (b2v > tau2) {
+      const float bf = sqrtf((float)b2v);
+      scp = sc;
+      sc = 1.0f / bf;
+      bprev = bf;
+      v = w * sc;
+    } else {
+      // Breakdown: restart from the column of P with the largest diagonal
+      // (cluster-wide argmax, ties to the smaller row), published into vb[nxt].
+      status |= SET_BREAKDOWN;
+      unsigned long long kk = 0ull;
+      if (r < k && r >= c0 && r < c0 + CPT) {
+        float d = 0.f;
+#pragma unroll
+        for (int c = 0; c < CPT; c += 2) {
+          if (c0 + c == r) d = Pr[c / 2].x;
+          if (c0 + c + 1 == r) d = Pr[c / 2].y;
+        }
+        d = fmaxf(d, 0.f);
+        kk = ((unsigned long long)__float_as_uint(d) << 32) | (unsigned)(0x7fffffff - r);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long y2 = __shfl_xor_sync(0xffffffffu, kk, o);
+        kk = y2 > kk ? y2 : kk;
+      }
+      if ((t & 31) == 0) sm.red[t >> 5] = __longlong_as_double((long long)kk);
+      __syncthreads();
+      if (t < CS) {
+        unsigned long long m = 0;
+        for (int i = 0; i < NTC / 32; ++i) {
+          const unsigned long long y2 = (unsigned long long)__double_as_longlong(sm.red[i]);
+          m = y2 > m ? y2 : m;
+        }
+        cl.map_shared_rank(&sm, (unsigned)t)->key[rank] = m;
+      }
+      cl.sync();
+      unsigned long long best = 0;
+#pragma unroll
+      for (int q = 0; q < CS; ++q) best = sm.key[q] > best ? sm.key[q] : best;
+      const int mrow = 0x7fffffff - (int)(best & 0xffffffffu);
+      if (mrow / R == rank && lr == mrow % R) {
+#pragma unroll
+        for (int q = 0; q < CS; ++q) {
+          float* dst = cl.map_shared_rank(&sm, (unsigned)q)->vb[nxt];
+#pragma unroll
+          for (int c = 0; c < CPT; c += 2) {
+            dst[c0 + c] = Pr[c / 2].x;
+            dst[c0 + c + 1] = Pr[c / 2].y;
+          }
+        }
+      }
+      cl.sync();
+      const float z = sm.vb[nxt][r];
+      const double zz = cluster_sum<KB, CS, NTC>(lead ? (double)z * (double)z : 0.0, sm, 2, cl, rank);
+      if (t == 0 && rank == 0) sm.ab[j + 1].y = 0x1p-600;  // decoupled block (see sturm_count)
+      scp = sc;
+      sc = 1.0f / sqrtf((float)zz);
+      bprev = 0.f;
+      v = z * sc;
+    }
+    const int old_prv = prv;
+    prv = cur;
+    cur = nxt;
+    nxt = old_prv;
+  }
+  cl.sync();  // every rank done with the step loop before T is read
+
+  // ---- extremes on rank 0: warp 0 lambda_min, warp 1 lambda_max, 33-way -----
+  if (rank == 0) {
+    if (status & SET_NONFINITE) {
+      if (t == 0) write_failed(out, set, 0, 0, status);
+    } else {
+      double glo = 1e300, ghi = -1e300;
+      if (t < 64) {
+        for (int i = t & 31; i < k; i += 32) {
+          const double rad = (i > 0 ? sqrt(sm.ab[i].y) : 0.0) + (i + 1 < k ? sqrt(sm.ab[i + 1].y) : 0.0);
+          glo = fmin(glo, sm.ab[i].x - rad);
+          ghi = fmax(ghi, sm.ab[i].x + rad);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          glo = fmin(glo, __shfl_xor_sync(0xffffffffu, glo, o));
+          ghi = fmax(ghi, __shfl_xor_sync(0xffffffffu, ghi, o));
+        }
+        const double pad = 0x1p-51 * fmax(fabs(glo), fabs(ghi)) + 1e-300;
+        const double e = multisect_warp(sm.ab, k, glo - pad, ghi + pad, t < 32 ? 1 : k);
+        if ((t & 31) == 0) sm.part[2][t >> 5] = e;
+      }
+      __syncthreads();
+      if (t == 0) {
+        const double lmin = sm.part[2][0], lmax = sm.part[2][1];
+        if (out.lmin) out.lmin[set] = lmin;
+        if (out.lmax) out.lmax[set] = lmax;
+        if (out.delta) out.delta[set] = fmax(1.0 - lmin, lmax - 1.0);
+        if (out.err) out.err[set] = status;
+      }
+    }
+  }
+  cl.sync();  // rank 0's reads of T and part[] precede the next set's writes
+}
+
+}  // namespace pl

@@ -2,6 +2,7 @@
 // includes this: pl_api.cu).
 #pragma once
 #include "pl_cgs.cuh"
+#include "pl_cluster.cuh"
 #include "pl_engine.cuh"
 #include "pl_engine_sa.cuh"
 #include "pl_indexgen.cuh"
@@ -177,9 +178,36 @@ __global__ void __launch_bounds__(256, 1)
 }
 
 // ---------------------------------------------------------------------------
+// Large-k batched form on thread-block clusters (pl_cluster.cuh): persistent,
+// one set per cluster of CS CTAs at a time.
+// ---------------------------------------------------------------------------
+template <int KB, int CS, int NTC>
+__global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(NTC, 1)
+    k_cluster_solve(MatrixF32 M, SetSource src, SetOutputs out) {
+  extern __shared__ __align__(16) float dsm[];
+  ClusterSmem<KB, CS, NTC>& sm = *reinterpret_cast<ClusterSmem<KB, CS, NTC>*>(dsm);
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const long long ncl = gridDim.x / CS;
+  const long long cid = blockIdx.x / CS;
+  const long long nitems = item_count(src);
+  const int pbase = src.perm_start ? *src.perm_start : 0;
+  for (long long it = cid; it < nitems; it += ncl) {  // the same items on every rank
+    long long set, off;
+    int k;
+    set_span(src, it, pbase, set, off, k);
+    if (k < 1 || k > KB) {
+      if (rank == 0 && threadIdx.x == 0) write_failed(out, set, off, 0, SET_BAD_K);
+      continue;
+    }
+    cluster_solve_set<KB, CS, NTC>(M, src.idx + off, k, set, out, sm, cl, rank);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Binning of a CSR set list by k (device-side counting sort of set ids).
 // ---------------------------------------------------------------------------
-constexpr int kMaxBins = 8;
+constexpr int kMaxBins = 12;
 
 struct BinTable {
   int nb;

@@ -303,13 +303,12 @@ def test_solve_host_equals_device():
 
 
 def test_tuning_variants_agree():
-    A = cached_gram(1024, 4096)
+    A = cached_gram(2048, 4096)
     for b in range(api.num_bins()):
         kmax = api.bin_kmax(b)
-        if kmax > 128:
-            continue
         k = kmax
-        o, idx = O.gen_stream(14, 0, 64, 4096, 0, k, k)
+        nsets = 64 if kmax <= 128 else 6
+        o, idx = O.gen_stream(14, 0, nsets, 4096, 0, k, k)
         nvar, _ = api.tune_describe(b, 0)
         outs = []
         for v in range(nvar):
