@@ -127,6 +127,19 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
+def tuned_variant(b: int) -> int:
+    """Variant of bin b the autotuner chose for this GPU (0 = compiled default)."""
+    p = os.path.join(ROOT, "paralanczos_b200", "tuning.json")
+    try:
+        import torch
+        data = json.load(open(p))
+        if data.get("device") == torch.cuda.get_device_name():
+            return int(data["bins"][str(b)]["variant"])
+    except Exception:
+        pass
+    return 0
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -328,7 +341,7 @@ def run_ours(args):
             "accuracy": {"sets_checked": chk, "max_rel_err_vs_dsyev": max_rel},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
                          "frac": achieved / peak_fp32, "traffic": traffic,
-                         "kernel": "k_reg_solve<64,1,1,128,3>",
+                         "kernel": api.tune_describe(3, tuned_variant(3))[1],
                          "peak_source": "FP32 FMA peak measured live by k_fma_peak (no FP32 figure in "
                                         "MEASURED_PEAKS.json)",
                          "algorithmic": "4k^3 FLOP per set (k matvecs + one reorthogonalisation pass)"},

@@ -70,6 +70,9 @@ def lib():
             f.restype = res
             f.argtypes = args
         _lib = L
+        # launch shapes chosen by the autotuner for this GPU, when present
+        from . import autotune
+        autotune.apply(lib=L)
     return _lib
 
 

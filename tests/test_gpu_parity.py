@@ -320,3 +320,16 @@ def test_tuning_variants_agree():
             for s, t in enumerate(truth):
                 assert abs(r["lmin"][s] - t[0]) <= RTOL * t[0]
                 assert abs(r["lmax"][s] - t[-1]) <= RTOL * t[-1]
+
+
+def test_rip_sweep_on_gpu_matches_oracle():
+    import torch
+    from paralanczos_b200.sweep import gpu_solver, rip_sweep
+    A = cached_gram(128, 512)
+    At = dev(A)
+    r = rip_sweep(gpu_solver(At, 512, 16, seed=21), 3000, chunk=1000)
+    _, idx = O.gen_stream(21, 0, 3000, 512, 0, 16, 16)
+    ref = O.batch(A, idx, k=16)
+    i = int(np.argmax(ref["delta"]))
+    assert r.set_id == i and r.n_solved == 3000
+    assert abs(r.delta - ref["delta"][i]) <= RTOL * abs(ref["delta"][i])
