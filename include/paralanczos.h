@@ -114,6 +114,32 @@ long long pl_gen_stream_host(unsigned long long seed, long long first, long long
 /* FP64 -> FP32 conversion on the device (for FP64 matrices). */
 int pl_convert_f64_f32(const double *in, float *out, long long count, void *stream);
 
+/* ---- on-the-fly Gram form ------------------------------------------------
+ * A is never materialised: each A[S,S] = Phi_S^T Phi_S is formed on the
+ * tensor cores (bf16 split of the FP32 frame, FP32 accumulation, exactly
+ * symmetric result) and solved like pl_solve.  Spec: the reference's Gram
+ * kernels DSG_B / DSG_B1 / SG_B1 (ParaLanczos.cu:364-438, declared
+ * ParaLanczos.h:24-28), which form subgrams[i*n+j] = sum_k
+ * Frame[S_i + k*N] Frame[S_j + k*N] from a row-major M x N frame; no wrapper
+ * of the reference calls them.  Uniform k, 1 <= k <= 128.                    */
+/* Bytes of the prepared frame for an m x n Phi (m rows = Gram inner dim.).  */
+long long pl_gram_prep_bytes(int m, int n);
+/* Prepare the frame once: Phi is the reference's row-major m x n frame
+ * (device, FP32, row stride ld >= n); prep receives pl_gram_prep_bytes bytes
+ * (device, 16-byte aligned).  Asynchronous on `stream`.                      */
+int pl_gram_prepare(const float *Phi, long long ld, int m, int n, void *prep, void *stream);
+/* The Gram blocks themselves: blocks[s*k*k + i*k + j] = (Phi_S^T Phi_S)_ij
+ * (device FP32), err[s] = PL_SET_BAD_INDEX for a set with an index outside
+ * [0, n).  Synchronous (returns PL_ETIMEDOUT if a bounded wait gave up).     */
+int pl_gram_blocks(const void *prep, int m, int n, const int *idx, long long nsets, int k,
+                   float *blocks, int *err, void *stream);
+/* Form and solve: outputs as pl_solve (device pointers; eig at s*k).  Works
+ * in chunks through a cached device buffer of at most PL_GRAM_CHUNK_MB
+ * (default 2048) MiB of blocks.  Synchronous like pl_gram_blocks.           */
+int pl_solve_gram(const void *prep, int m, int n, const int *idx, long long nsets, int k,
+                  int form, double *lmin, double *lmax, double *delta, int *err, double *eig,
+                  double *det, void *stream);
+
 /* ---- ParaLanczos.h drop-ins with a status return ------------------------ */
 /* Host pointers, FP64 matrix, all eigenvalues out; semantics of the named
  * reference routine (validation messages, output layout).  PL_STRICT=0 in the

@@ -76,6 +76,8 @@ def lib():
         L.orc_gershgorin.argtypes = [_dp, _dp, C.c_int, _dp, _dp]
         L.orc_gershgorin.restype = None
         L.orc_bisect_all.argtypes = [_dp, _dp, C.c_int, _dp]
+        L.orc_dsg_b.restype = None
+        L.orc_dsg_b.argtypes = [_dp, _dp, C.c_int, C.c_int, _ip, C.c_int, C.c_int]
         L.orc_bisect_all.restype = None
         _lib = L
     return _lib
@@ -229,6 +231,17 @@ def bisect_all(alpha, beta2):
     eig = np.zeros(len(alpha))
     lib().orc_bisect_all(_d(alpha), _d(beta2), len(alpha), _d(eig))
     return eig
+
+
+def dsg_b(frame, subset, off: int = 0):
+    """FP64 Gram block of frame columns `subset` (DSG_B, ParaLanczos.cu:364-382)."""
+    frame = np.ascontiguousarray(frame, dtype=np.float64)
+    subset = np.ascontiguousarray(subset, dtype=np.int32)
+    M, N = frame.shape
+    n = len(subset)
+    out = np.zeros((n, n))
+    lib().orc_dsg_b(_d(out), _d(frame), M, N, _i(subset), n, off)
+    return out
 
 
 # ----------------------------------------------------------------------------- LAPACK truth

@@ -25,6 +25,10 @@
  *                          (the reference has none; its callers hand in
  *                          subIndex, ParaLanczos.cu:1843-1845).  Same bits as
  *                          the device generator in paralanczos_b200/csrc.
+ *   - orc_dsg_b          : the subset Gram kernel DSG_B, ParaLanczos.cu:364-382
+ *                          (subgrams[j + i*n] = sum_k Frame[S_i + k*N + off] *
+ *                          Frame[S_j + k*N + off], FP64, k ascending), the spec
+ *                          of the on-the-fly Gram form.
  *   - orc_sturm_count /
  *     orc_bisect_*       : the FP64 Sturm-count bisection the GPU path uses in
  *                          place of TQLRAT (the reference's only Sturm code,
@@ -393,4 +397,20 @@ void orc_bisect_all(const double *alpha, const double *beta2, int k, double *eig
     double lo, hi;
     orc_gershgorin(alpha, beta2, k, &lo, &hi);
     for (int m = 0; m < k; ++m) eig[m] = orc_bisect_one(alpha, beta2, k, m, lo, hi);
+}
+
+/* ------------------------------------------------------------------------- */
+/* DSG_B restated (ParaLanczos.cu:364-382): the n x n Gram block of the frame */
+/* columns `subset` (row-major M x N frame, column offset `off`), FP64 sums   */
+/* over the frame rows in ascending order.                                    */
+void orc_dsg_b(double *subgram, const double *frame, int M, int N, const int *subset, int n, int off)
+{
+    for (int i = 0; i < n; ++i) {
+        for (int j = 0; j < n; ++j) {
+            double val = 0.0;
+            for (int k = 0; k < M; ++k)
+                val += frame[subset[i] + (long long)k * N + off] * frame[subset[j] + (long long)k * N + off];
+            subgram[j + i * n] = val;
+        }
+    }
 }

@@ -42,6 +42,10 @@ SIGNATURES = {
     "pl_bin_kmax": (_i, [_i]),
     "pl_fp32_peak": (_i, [C.POINTER(_d), _vp]),
     "pl_release": (_i, []),
+    "pl_gram_prep_bytes": (_ll, [_i, _i]),
+    "pl_gram_prepare": (_i, [_vp, _ll, _i, _i, _vp, _vp]),
+    "pl_gram_blocks": (_i, [_vp, _i, _i, _vp, _ll, _i, _vp, _vp, _vp]),
+    "pl_solve_gram": (_i, [_vp, _i, _i, _vp, _ll, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
 }
 
 _lib = None

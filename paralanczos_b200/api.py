@@ -204,3 +204,56 @@ def tune_set(b: int, variant: int) -> None:
 
 def release() -> None:
     check(lib().pl_release(), "pl_release")
+
+
+# --------------------------------------------------------------------------- on-the-fly Gram
+
+
+class GramFrame:
+    """A frame Phi (m x n, the reference's row-major Frame layout) prepared on
+    the device for the on-the-fly Gram form (bf16 hi/lo pieces per column).
+    The FP32 frame itself is not kept."""
+
+    def __init__(self, Phi, stream=None):
+        import torch
+        if Phi.dtype != torch.float32 or not Phi.is_cuda or Phi.dim() != 2 or Phi.stride(1) != 1:
+            raise TypeError("Phi must be a row-major 2-D float32 CUDA tensor")
+        self.m, self.n = int(Phi.shape[0]), int(Phi.shape[1])
+        nbytes = lib().pl_gram_prep_bytes(self.m, self.n)
+        self.prep = torch.empty(nbytes, dtype=torch.uint8, device=Phi.device)
+        st = stream if stream is not None else torch.cuda.current_stream(Phi.device)
+        check(lib().pl_gram_prepare(Phi.data_ptr(), Phi.stride(0), self.m, self.n, self.prep.data_ptr(),
+                                    st.cuda_stream), "pl_gram_prepare")
+
+    def blocks(self, idx, k: int, stream=None):
+        """(nsets, k, k) float32 Gram blocks Phi_S^T Phi_S and int32 status bits."""
+        import torch
+        nsets = idx.numel() // int(k)
+        out = torch.empty((nsets, k, k), dtype=torch.float32, device=self.prep.device)
+        err = torch.empty(nsets, dtype=torch.int32, device=self.prep.device)
+        st = stream if stream is not None else torch.cuda.current_stream(self.prep.device)
+        check(lib().pl_gram_blocks(self.prep.data_ptr(), self.m, self.n, idx.data_ptr(), nsets, int(k),
+                                   out.data_ptr(), err.data_ptr(), st.cuda_stream), "pl_gram_blocks")
+        return out, err
+
+    def solve(self, idx, k: int, form="batched", want_all=False, stream=None, out=None):
+        """Like ``solve`` with A = Phi^T Phi never materialised (1 <= k <= 128)."""
+        import torch
+        if idx.dtype != torch.int32 or not idx.is_cuda or not idx.is_contiguous():
+            raise TypeError("idx must be a contiguous int32 CUDA tensor")
+        nsets = idx.numel() // int(k)
+        dev = self.prep.device
+        if out is None:
+            out = dict(lmin=torch.empty(nsets, dtype=torch.float64, device=dev),
+                       lmax=torch.empty(nsets, dtype=torch.float64, device=dev),
+                       delta=torch.empty(nsets, dtype=torch.float64, device=dev),
+                       err=torch.empty(nsets, dtype=torch.int32, device=dev))
+            if want_all:
+                out["eig"] = torch.empty(nsets * int(k), dtype=torch.float64, device=dev)
+                out["det"] = torch.empty(nsets, dtype=torch.float64, device=dev)
+        st = stream if stream is not None else torch.cuda.current_stream(dev)
+        p = lambda name: out[name].data_ptr() if name in out and out[name] is not None else None
+        check(lib().pl_solve_gram(self.prep.data_ptr(), self.m, self.n, idx.data_ptr(), nsets, int(k),
+                                  FORMS[form], p("lmin"), p("lmax"), p("delta"), p("err"), p("eig"),
+                                  p("det"), st.cuda_stream), "pl_solve_gram")
+        return out

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/paralanczos.h"
+#include "pl_internal.h"
 #include "pl_kernels.cuh"
 
 using namespace pl;
@@ -511,6 +512,16 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 }  // namespace
 
+namespace pl {
+int api_solve_uniform(const MatrixF32& M, const int* idx, long long nsets, int k, int form,
+                      const SetOutputs& out, cudaStream_t st) {
+  return solve_uniform(M, idx, nsets, k, form, out, st);
+}
+std::mutex& api_mutex() { return g_mu; }
+void api_note_cuda(cudaError_t e) { g_last_cuda = (int)e; }
+int api_device_sms() { return device_sms(); }
+}  // namespace pl
+
 // =============================================================================
 // Allocation-free entry point (pl_solve_noalloc)
 // =============================================================================
@@ -727,6 +738,7 @@ int pl_release(void) {
     s->p = nullptr;
     s->bytes = 0;
   }
+  gram_release();
   return PL_OK;
 }
 

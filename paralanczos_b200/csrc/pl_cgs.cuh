@@ -41,7 +41,7 @@ __device__ __forceinline__ void cgs_solve_set(const MatrixF32& M, const int* __r
 
   bool bad = false;
   for (int c = t; c < k; c += NT) {
-    const int v = __ldg(S + c);
+    const int v = set_index(M, S, c);
     bad |= (v < 0) | (v >= M.n);
     sm.idx[c] = (v >= 0 && v < M.n) ? v : 0;
   }
@@ -55,7 +55,7 @@ __device__ __forceinline__ void cgs_solve_set(const MatrixF32& M, const int* __r
   // gather A[S,S] (column c, row i) into As; Frobenius norm
   double fro = 0.0;
   for (int c = 0; c < k; ++c) {
-    const float* __restrict__ arow = M.A + (size_t)sm.idx[c] * (size_t)M.lda;  // row S_c = column S_c
+    const float* __restrict__ arow = set_base(M, set) + (size_t)sm.idx[c] * (size_t)M.lda;  // row S_c = column S_c
     for (int i = t; i < k; i += NT) {
       const float a = __ldg(arow + sm.idx[i]);
       As[(size_t)c * lda + i] = a;

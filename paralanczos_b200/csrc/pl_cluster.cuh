@@ -94,7 +94,7 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
   for (int c = t; c < KB; c += NTC) {
     int v = 0;
     if (c < k) {
-      v = __ldg(S + c);
+      v = set_index(M, S, c);
       bad |= (v < 0) | (v >= M.n);
     }
     sm.idx[c] = (c < k && v >= 0 && v < M.n) ? v : 0;
@@ -112,7 +112,7 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
   double fro = 0.0;
   {
     const bool rv = r < k;
-    const float* __restrict__ arow = M.A + (size_t)sm.idx[r] * (size_t)M.lda;
+    const float* __restrict__ arow = set_base(M, set) + (size_t)sm.idx[r] * (size_t)M.lda;
 #pragma unroll
     for (int ch = 0; ch < NCH; ++ch) {
       float e[4];

@@ -42,7 +42,21 @@ struct MatrixF32 {
   const float* A;  // symmetric, row-major
   long long lda;
   int n;
+  // > 0: A holds one already-formed k x k block per set (row stride lda) at
+  // A + set * set_stride, indexed locally 0..k-1 (the on-the-fly Gram form);
+  // n is then the block dimension.
+  long long set_stride = 0;
 };
+
+// Row/column of the matrix the engines read for position c of the set.
+__device__ __forceinline__ int set_index(const MatrixF32& M, const int* __restrict__ S, int c) {
+  return M.set_stride ? c : __ldg(S + c);
+}
+
+// Base of the matrix the set's rows are read from.
+__device__ __forceinline__ const float* set_base(const MatrixF32& M, long long set) {
+  return M.set_stride ? M.A + set * M.set_stride : M.A;
+}
 
 __device__ __forceinline__ long long item_count(const SetSource& src) {
   return src.count ? (long long)(*src.count) : src.nitems;

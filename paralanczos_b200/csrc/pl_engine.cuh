@@ -190,7 +190,7 @@ __device__ __forceinline__ int solve_set(const MatrixF32& M, const int* __restri
   for (int c = t; c < KB; c += NT) {
     int v = 0;
     if (c < k) {
-      v = __ldg(S + c);
+      v = set_index(M, S, c);
       bad |= (v < 0) | (v >= M.n);
     }
     sm.idx[c] = (c < k && v >= 0 && v < M.n) ? v : 0;
@@ -213,7 +213,7 @@ __device__ __forceinline__ int solve_set(const MatrixF32& M, const int* __restri
     const int r = rs + q * C::RSLOTS;
     rowid[q] = r;
     const bool rv = r < k;
-    const float* __restrict__ arow = M.A + (size_t)sm.idx[r] * (size_t)M.lda;
+    const float* __restrict__ arow = set_base(M, set) + (size_t)sm.idx[r] * (size_t)M.lda;
 #pragma unroll
     for (int cc = 0; cc < CPT; cc += 2) {
       const int c = c0 + cc;

@@ -1,0 +1,667 @@
+// pl_gram.cu -- on-the-fly Gram form: A[S,S] = Phi_S^T Phi_S on the tcgen05
+// tensor cores, then the subset Lanczos on the formed blocks.
+//
+// The reference's Gram kernels (DSG_B, ParaLanczos.cu:364-382; DSG_B1 and
+// SG_B1, ParaLanczos.cu:388-438) form subgrams[i*n+j] = sum_k
+// Frame[S_i + k*N + off] * Frame[S_j + k*N + off] from a row-major M x N
+// "frame" in FP64 scalar code; no wrapper calls them.  Here the frame is
+// prepared once into a column-major bf16 pair layout and every set's Gram
+// block is one 128 x 128 x M batched GEMM on the 5th-generation tensor cores:
+//
+//   x = hi + lo,  hi = bf16(x),  lo2 = bf16(2 (x - hi))       (exact split)
+//   D1 = hi hi^T + hi lo2^T,  D2 = lo2 lo2^T                   (FP32 in TMEM)
+//   A_S = (F + F^T) / 2,  F = D1 + D2 / 4
+//       = hi hi^T + hi lo^T + lo hi^T + lo lo^T
+//
+// i.e. three bf16 products per K step (the budget of the usual bf16x3 split),
+// with the cross terms folded by symmetry so that the lo lo^T term fits in the
+// same budget; the result is exactly symmetric.  The only lost bits are the
+// residual x - hi - lo (below 2^-16 |x|).
+//
+// Kernel structure (one persistent CTA per SM, 288 threads):
+//   warps 0-3  gather: cp.async of the set's 128 column records per 64-row
+//              K chunk into a 4-stage ring of SWIZZLE_128B K-major tiles;
+//   warp  8    owns 512 TMEM columns, one elected thread issues tcgen05.mma
+//              and tcgen05.commit;
+//   warps 4-7  epilogue: tcgen05.ld of the accumulators (warp w reads TMEM
+//              lanes 32 (w % 4) ...), symmetrise through shared memory and
+//              write the k x k FP32 block coalesced.
+// The tensor core's FP32 accumulation does not round to nearest: a sum of
+// many same-sign terms (the diagonal, sum of squares) drifts by about one
+// unit in the last place per accumulation step.  D1 is therefore accumulated
+// in segments of SEG chunks (256 rows of Phi, 32 steps), each into a fresh
+// TMEM buffer (two, ping-pong), and the epilogue adds the segments with
+// round-to-nearest FP32 adds; D2 (2^-16 of the result) spans the whole set.
+// Every mbarrier wait is bounded (%globaltimer); a wait that gives up sets a
+// CTA-wide abort flag and a device status word, every role leaves its loop,
+// outstanding copies and MMAs are drained and TMEM is freed before return.
+// No TMA and no cluster multicast is used.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+
+#include "../../include/paralanczos.h"
+#include "pl_common.cuh"
+#include "pl_internal.h"
+
+namespace pl {
+namespace gram {
+
+constexpr int KCH = 64;                       // rows of Phi (K) per stage
+constexpr int ROWS = 128;                     // set positions per tile (UMMA M = N)
+constexpr int REC_BYTES = 2 * KCH * 2;        // one column's (hi, lo2) record of a chunk
+constexpr int PIECE_BYTES = ROWS * KCH * 2;   // one bf16 piece of a stage: 16 KB
+constexpr int STAGE_BYTES = 2 * PIECE_BYTES;  // hi + lo2
+constexpr int NS = 4;                         // ring stages
+constexpr int LAG = 3;                        // cp.async groups a gather thread keeps in flight
+constexpr int EPAD = ROWS + 1;                // epilogue staging row stride (floats)
+constexpr int NPROD = 128;
+constexpr int NEPI = 128;
+constexpr int NTHREADS = NPROD + NEPI + 32;
+constexpr int SEG = 4;                        // chunks (256 rows of Phi) per D1 segment
+constexpr int TMEM_COLS = 512;                // D1 segment ping-pong + D2 per set, x 2
+constexpr unsigned long long kWaitNs = 2000000000ull;  // bounded waits: 2 s
+
+struct SmemLayout {
+  static constexpr int ring = 0;
+  static constexpr int epi = NS * STAGE_BYTES;
+  static constexpr int bars = epi + ROWS * EPAD * 4;
+  // full[NS], empty[NS], segfull[2], segempty[2], d2full[2], d2empty[2], fin
+  static constexpr int nbars = 2 * NS + 9;
+  static constexpr int misc = bars + nbars * 8;  // tmem base, abort, epilogue go flags
+  static constexpr int total = misc + 32;
+};
+constexpr size_t kSmemBytes = SmemLayout::total + 1024;  // + alignment slack
+
+// Instruction descriptor of tcgen05.mma kind::f16: D FP32, A and B bf16, both
+// K-major, M = N = 128 (PTX ISA "Instruction descriptor" table).
+constexpr uint32_t kIdesc = (1u << 4)            // D format: F32
+                            | (1u << 7)          // A format: BF16
+                            | (1u << 10)         // B format: BF16
+                            | ((128u >> 3) << 17)  // N >> 3
+                            | ((128u >> 4) << 24);  // M >> 4
+
+// Shared-memory matrix descriptor of a K-major SWIZZLE_128B tile whose 8-row
+// groups are 1024 B apart; the leading offset is unused by this layout.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = (uint64_t)((saddr & 0x3FFFFu) >> 4);
+  d |= (uint64_t)1 << 16;            // leading byte offset (ignored)
+  d |= (uint64_t)(1024 >> 4) << 32;  // stride byte offset
+  d |= (uint64_t)1 << 46;            // descriptor version (sm_100)
+  d |= (uint64_t)2 << 61;            // SWIZZLE_128B
+  return d;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for the phase with the given parity.  false: gave up (timeout
+// here, or another role already aborted); the abort flag is then set.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort,
+                                          int* status) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = globaltimer();
+  for (uint32_t i = 1;; ++i) {
+    if (mbar_try(bar, parity)) return true;
+    if ((i & 31) == 0) {
+      if (*abort) return false;
+      if (globaltimer() - t0 > kWaitNs) {
+        *abort = 1;
+        atomicExch(status, 1);
+        return false;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(tmem_d), "l"(da), "l"(db), "r"(kIdesc), "r"(acc)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+
+// 32 consecutive FP32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+        "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+        "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Preparation: row-major M x N frame (the reference's Frame[S_i + k*N]) ->
+// per column c and 64-row chunk kc a 256-byte record {hi[64], lo2[64]} at
+// prep + (c * KC + kc) * 256, rows >= M zero.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_gram_split(const float* __restrict__ Phi, long long ld,
+                                                    int m, int n, int kc_total,
+                                                    __nv_bfloat16* __restrict__ prep) {
+  __shared__ float tile[KCH][KCH + 1];
+  const int n0 = blockIdx.x * KCH;
+  const int kc = blockIdx.y;
+  const int m0 = kc * KCH;
+  for (int e = threadIdx.x; e < KCH * KCH; e += 256) {
+    const int r = e / KCH, c = e % KCH;
+    const int gm = m0 + r, gn = n0 + c;
+    tile[r][c] = (gm < m && gn < n) ? Phi[(size_t)gm * ld + gn] : 0.f;
+  }
+  __syncthreads();
+  // 64 columns x 16 pieces of 8 bf16 (16 B): piece p < 8 holds hi of rows
+  // 8p..8p+7, piece p >= 8 lo2 of rows 8(p-8)..
+  for (int e = threadIdx.x; e < KCH * 16; e += 256) {
+    const int c = e / 16, p = e % 16;
+    const int gn = n0 + c;
+    if (gn >= n) continue;
+    const int rb = (p & 7) * 8;
+    __align__(16) __nv_bfloat16 out[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const float x = tile[rb + u][c];
+      const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+      out[u] = p < 8 ? hi : __float2bfloat16_rn(2.f * (x - __bfloat162float(hi)));
+    }
+    char* rec = (char*)prep + ((size_t)gn * kc_total + kc) * REC_BYTES;
+    *(uint4*)(rec + p * 16) = *(const uint4*)out;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Batched Gram blocks of sets [0, nsets) (uniform k <= 128): block s at
+// blocks + s * k * k, row-major, exactly symmetric.  gerr[s] |= SET_BAD_INDEX
+// for a set with an index outside [0, n) (its rows read as zero).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(NTHREADS, 1)
+    k_gram(const char* __restrict__ prep, int n, int kc_total, const int* __restrict__ idx,
+           long long nsets, int k, float* __restrict__ blocks, int* __restrict__ gerr,
+           int* __restrict__ status) {
+  extern __shared__ unsigned char smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  unsigned char* sbase = smem_raw + (base - raw);
+  float* E = (float*)(sbase + SmemLayout::epi);
+  const uint32_t bar0 = base + SmemLayout::bars;
+  auto full_bar = [&](int s) { return bar0 + 8u * s; };
+  auto empty_bar = [&](int s) { return bar0 + 8u * (NS + s); };
+  auto segfull_bar = [&](int b) { return bar0 + 8u * (2 * NS + b); };
+  auto segempty_bar = [&](int b) { return bar0 + 8u * (2 * NS + 2 + b); };
+  auto d2full_bar = [&](int a) { return bar0 + 8u * (2 * NS + 4 + a); };
+  auto d2empty_bar = [&](int a) { return bar0 + 8u * (2 * NS + 6 + a); };
+  const uint32_t fin_bar = bar0 + 8u * (2 * NS + 8);
+  uint32_t* tmem_slot = (uint32_t*)(sbase + SmemLayout::misc);
+  volatile int* abort = (volatile int*)(sbase + SmemLayout::misc + 4);
+  volatile int* epi_go = (volatile int*)(sbase + SmemLayout::misc + 8);  // [2]
+  volatile int* go_d2 = (volatile int*)(sbase + SmemLayout::misc + 16);
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  if (tid == 0) {
+    for (int s = 0; s < NS; ++s) {
+      mbar_init(full_bar(s), NPROD);
+      mbar_init(empty_bar(s), 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(segfull_bar(a), 1);
+      mbar_init(segempty_bar(a), NEPI);
+      mbar_init(d2full_bar(a), 1);
+      mbar_init(d2empty_bar(a), NEPI);
+    }
+    mbar_init(fin_bar, 1);
+    *abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 8) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const size_t rec_stride = (size_t)kc_total * REC_BYTES;
+
+  if (warp < 4) {
+    // ---------------- gather ----------------
+    const int rsub = tid >> 4;  // 0..7: row within each 8-row group
+    const int sg = tid & 15;    // 16-byte segment of the 256-byte record
+    const uint32_t dst0 = (uint32_t)((sg >> 3) * PIECE_BYTES + rsub * 128 + (((sg & 7) ^ rsub) << 4));
+    uint32_t it = 0;
+    bool ok = true;
+    for (long long set = blockIdx.x; set < nsets && ok; set += gridDim.x) {
+      const char* src[16];
+      uint32_t nbytes = 0;  // 16 if row valid else 0 (zero fill), one bit per row
+      bool bad = false;
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int r = rsub + 8 * i;
+        int v = 0;
+        bool valid = false;
+        if (r < k) {
+          v = __ldg(idx + set * (long long)k + r);
+          valid = v >= 0 && v < n;
+          bad |= !valid;
+        }
+        src[i] = prep + (valid ? (size_t)v * rec_stride : 0) + sg * 16;
+        nbytes |= (valid ? 1u : 0u) << i;
+      }
+      if (bad) atomicOr(gerr + set, SET_BAD_INDEX);
+      for (int kc = 0; kc < kc_total; ++kc, ++it) {
+        const int s = it % NS;
+        if (it >= NS && !mbar_wait(empty_bar(s), ((it / NS) - 1) & 1, abort, status)) {
+          ok = false;
+          break;
+        }
+        const uint32_t dst = base + SmemLayout::ring + s * STAGE_BYTES + dst0;
+        const size_t koff = (size_t)kc * REC_BYTES;
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+          cp_async16(dst + i * 1024, src[i] + koff, ((nbytes >> i) & 1u) * 16u);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        if (it >= LAG - 1) {
+          asm volatile("cp.async.wait_group %0;" ::"n"(LAG - 1) : "memory");
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          mbar_arrive(full_bar((it - (LAG - 1)) % NS));
+        }
+      }
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    if (ok) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      for (uint32_t u = it >= (uint32_t)(LAG - 1) ? it - (LAG - 1) : 0; u < it; ++u)
+        mbar_arrive(full_bar(u % NS));
+    }
+  } else if (warp == 8) {
+    // ---------------- MMA issue (one thread) ----------------
+    if ((tid & 31) == 0) {
+      uint32_t it = 0, j = 0, G = 0;
+      bool ok = true;
+      for (long long set = blockIdx.x; set < nsets && ok; set += gridDim.x, ++j) {
+        const uint32_t a = j & 1;
+        if (j >= 2 && !mbar_wait(d2empty_bar(a), ((j >> 1) - 1) & 1, abort, status)) {
+          ok = false;
+          break;
+        }
+        const uint32_t d2 = tmem + 256 + a * 128;
+        for (int kc0 = 0; kc0 < kc_total && ok; kc0 += SEG, ++G) {
+          const uint32_t b = G & 1;
+          if (G >= 2 && !mbar_wait(segempty_bar(b), ((G >> 1) - 1) & 1, abort, status)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t d1 = tmem + b * 128;
+          const int kend = kc0 + SEG < kc_total ? kc0 + SEG : kc_total;
+          for (int kc = kc0; kc < kend; ++kc, ++it) {
+            const int s = it % NS;
+            if (!mbar_wait(full_bar(s), (it / NS) & 1, abort, status)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t hi = base + SmemLayout::ring + s * STAGE_BYTES;
+            const uint64_t dh = sw128_desc(hi);
+            const uint64_t dl = sw128_desc(hi + PIECE_BYTES);
+#pragma unroll
+            for (int kk = 0; kk < KCH / 16; ++kk) {
+              const uint32_t acc1 = (kc != kc0 || kk) ? 1u : 0u;  // segment starts fresh
+              const uint32_t acc2 = (kc | kk) ? 1u : 0u;          // D2 spans the set
+              const uint64_t o = (uint64_t)(kk * 32) >> 4;         // 16 bf16 = 32 B along K
+              umma_bf16(d1, dh + o, dh + o, acc1);
+              umma_bf16(d1, dh + o, dl + o, 1u);
+              umma_bf16(d2, dl + o, dl + o, acc2);
+            }
+            umma_commit(empty_bar(s));
+          }
+          if (ok) umma_commit(segfull_bar(b));
+        }
+        if (ok) umma_commit(d2full_bar(a));
+      }
+      // drain: every MMA issued above has completed once this phase completes
+      umma_commit(fin_bar);
+      volatile int never = 0;
+      mbar_wait(fin_bar, 0, &never, status);
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue (warps 4-7) ----------------
+    // One thread waits on each barrier and broadcasts the outcome through a
+    // flag behind a named barrier, so all 128 threads leave together.
+    const int e = tid - NPROD;
+    const int q = warp & 3;
+    const int row = 32 * q + (tid & 31);
+    const uint32_t lane_base = tmem + ((uint32_t)(32 * q) << 16);
+    float* Er = E + row * EPAD;
+    uint32_t j = 0, G = 0;
+    bool ok = true;
+    for (long long set = blockIdx.x; set < nsets && ok; set += gridDim.x, ++j) {
+      const uint32_t a = j & 1;
+      // D1 segments: sum into this thread's row of E with round-to-nearest adds
+      for (int kc0 = 0; kc0 < kc_total; kc0 += SEG, ++G) {
+        const uint32_t b = G & 1;
+        if (e == 0) epi_go[b] = mbar_wait(segfull_bar(b), (G >> 1) & 1, abort, status) ? 1 : 0;
+        asm volatile("bar.sync 1, %0;" ::"n"(NEPI) : "memory");
+        if (!epi_go[b]) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+#pragma unroll 1
+        for (int cb = 0; cb < ROWS / 32; ++cb) {
+          float u[32];
+          tmem_ld32(lane_base + b * 128 + 32 * cb, u);
+          tmem_wait_ld();
+          if (kc0 == 0) {
+#pragma unroll
+            for (int c = 0; c < 32; ++c) Er[32 * cb + c] = u[c];
+          } else {
+#pragma unroll
+            for (int c = 0; c < 32; ++c) Er[32 * cb + c] += u[c];
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(segempty_bar(b));
+      }
+      if (!ok) break;
+      // D2 (the lo2 lo2^T term, scaled by 1/4)
+      if (e == 0) *go_d2 = mbar_wait(d2full_bar(a), (j >> 1) & 1, abort, status) ? 1 : 0;
+      asm volatile("bar.sync 1, %0;" ::"n"(NEPI) : "memory");
+      if (!*go_d2) break;
+      tc_fence_after();
+#pragma unroll 1
+      for (int cb = 0; cb < ROWS / 32; ++cb) {
+        float w[32];
+        tmem_ld32(lane_base + 256 + a * 128 + 32 * cb, w);
+        tmem_wait_ld();
+#pragma unroll
+        for (int c = 0; c < 32; ++c) Er[32 * cb + c] = fmaf(0.25f, w[c], Er[32 * cb + c]);
+      }
+      tc_fence_before();
+      mbar_arrive(d2empty_bar(a));
+      asm volatile("bar.sync 1, %0;" ::"n"(NEPI) : "memory");
+      if (row < k) {
+        float* dst = blocks + (size_t)set * k * k + row;
+#pragma unroll 4
+        for (int c = 0; c < k; ++c)
+          dst[(size_t)c * k] = 0.5f * (Er[c] + E[c * EPAD + row]);
+      }
+      asm volatile("bar.sync 1, %0;" ::"n"(NEPI) : "memory");
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 8) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS)
+                 : "memory");
+  }
+}
+
+// Sets flagged by the Gram kernel (bad index) report like the Lanczos
+// kernels' own validation: NaN results and the status bit.
+__global__ void k_gram_fixup(const int* __restrict__ gerr, long long nsets, SetOutputs out, int k,
+                             bool all) {
+  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nsets;
+       s += (long long)gridDim.x * blockDim.x) {
+    const int g = gerr[s];
+    if (!g) continue;
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    if (out.lmin) out.lmin[s] = nan;
+    if (out.lmax) out.lmax[s] = nan;
+    if (out.delta) out.delta[s] = nan;
+    if (out.det) out.det[s] = nan;
+    if (out.err) out.err[s] = g;
+    if (all && out.eig)
+      for (int m = 0; m < k; ++m) out.eig[s * k + m] = nan;
+  }
+}
+
+struct GramState {
+  void* blocks = nullptr;
+  size_t blocks_bytes = 0;
+  int* gerr = nullptr;
+  size_t gerr_count = 0;
+  int* status = nullptr;
+};
+GramState g_gram[64];
+
+GramState& gstate() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  return g_gram[dev < 0 || dev >= 64 ? 0 : dev];
+}
+
+int grow(void*& p, size_t& have, size_t need) {
+  if (have >= need) return PL_OK;
+  if (p) {
+    cudaDeviceSynchronize();
+    cudaFree(p);
+    p = nullptr;
+    have = 0;
+  }
+  cudaError_t e = cudaMalloc(&p, need);
+  if (e != cudaSuccess) {
+    api_note_cuda(e);
+    return e == cudaErrorMemoryAllocation ? PL_ENOMEM : PL_ECUDA;
+  }
+  have = need;
+  return PL_OK;
+}
+
+size_t chunk_bytes() {
+  static size_t b = [] {
+    const char* e = getenv("PL_GRAM_CHUNK_MB");
+    const long long mb = e ? atoll(e) : 2048;
+    return (size_t)(mb > 16 ? mb : 16) << 20;
+  }();
+  return b;
+}
+
+#define GCU(call)                                                         \
+  do {                                                                    \
+    cudaError_t e_ = (call);                                              \
+    if (e_ != cudaSuccess) {                                              \
+      api_note_cuda(e_);                                                  \
+      return e_ == cudaErrorMemoryAllocation ? PL_ENOMEM : PL_ECUDA;      \
+    }                                                                     \
+  } while (0)
+
+int launch_gram(const void* prep, int m, int n, const int* idx, long long nsets, int k, float* blocks,
+                int* gerr, int* status, cudaStream_t st) {
+  static bool attr = [] {
+    cudaFuncSetAttribute(k_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+    return true;
+  }();
+  (void)attr;
+  const int kc_total = (m + KCH - 1) / KCH;
+  long long grid = api_device_sms();
+  if (nsets < grid) grid = nsets;
+  k_gram<<<(unsigned)grid, NTHREADS, kSmemBytes, st>>>((const char*)prep, n, kc_total, idx, nsets, k,
+                                                       blocks, gerr, status);
+  GCU(cudaGetLastError());
+  return PL_OK;
+}
+
+int check_status(GramState& g, cudaStream_t st) {
+  int h = 0;
+  GCU(cudaMemcpyAsync(&h, g.status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  GCU(cudaStreamSynchronize(st));
+  return h ? PL_ETIMEDOUT : PL_OK;
+}
+
+int ensure_status(GramState& g, cudaStream_t st) {
+  if (!g.status) {
+    size_t have = 0;
+    void* p = nullptr;
+    int rc = grow(p, have, 256);
+    if (rc) return rc;
+    g.status = (int*)p;
+  }
+  GCU(cudaMemsetAsync(g.status, 0, sizeof(int), st));
+  return PL_OK;
+}
+
+int validate(const void* prep, int m, int n, const int* idx, long long nsets, int k) {
+  if (nsets < 0 || m < 1 || n < 1) return PL_EINVAL;
+  if (k < 1 || k > n) return PL_EINVAL;
+  if (k > ROWS) return PL_ENOTSUP;
+  if (nsets > 0 && (!prep || !idx)) return PL_EINVAL;
+  return PL_OK;
+}
+
+}  // namespace gram
+
+void gram_release() {
+  gram::GramState& g = gram::gstate();
+  if (g.blocks) cudaFree(g.blocks);
+  if (g.gerr) cudaFree(g.gerr);
+  if (g.status) cudaFree(g.status);
+  g = gram::GramState{};
+}
+
+}  // namespace pl
+
+using namespace pl;
+using namespace pl::gram;
+
+extern "C" {
+
+long long pl_gram_prep_bytes(int m, int n) {
+  if (m < 1 || n < 1) return -1;
+  const long long kc = (m + KCH - 1) / KCH;
+  return (long long)n * kc * REC_BYTES;
+}
+
+int pl_gram_prepare(const float* Phi, long long ld, int m, int n, void* prep, void* stream) {
+  if (!Phi || !prep || m < 1 || n < 1 || ld < n) return PL_EINVAL;
+  const int kc_total = (m + KCH - 1) / KCH;
+  dim3 grid((unsigned)((n + KCH - 1) / KCH), (unsigned)kc_total);
+  k_gram_split<<<grid, 256, 0, (cudaStream_t)stream>>>(Phi, ld, m, n, kc_total, (__nv_bfloat16*)prep);
+  GCU(cudaGetLastError());
+  return PL_OK;
+}
+
+int pl_gram_blocks(const void* prep, int m, int n, const int* idx, long long nsets, int k,
+                   float* blocks, int* err, void* stream) {
+  std::lock_guard<std::mutex> lk(api_mutex());
+  int rc = validate(prep, m, n, idx, nsets, k);
+  if (rc || nsets == 0) return rc;
+  if (!blocks || !err) return PL_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  GramState& g = gstate();
+  rc = ensure_status(g, st);
+  if (rc) return rc;
+  GCU(cudaMemsetAsync(err, 0, sizeof(int) * (size_t)nsets, st));
+  rc = launch_gram(prep, m, n, idx, nsets, k, blocks, err, g.status, st);
+  if (rc) return rc;
+  return check_status(g, st);
+}
+
+int pl_solve_gram(const void* prep, int m, int n, const int* idx, long long nsets, int k, int form,
+                  double* lmin, double* lmax, double* delta, int* err, double* eig, double* det,
+                  void* stream) {
+  std::lock_guard<std::mutex> lk(api_mutex());
+  int rc = validate(prep, m, n, idx, nsets, k);
+  if (rc || nsets == 0) return rc;
+  if (form != PL_FORM_BATCHED && form != PL_FORM_PLAIN) return PL_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  GramState& g = gstate();
+  const size_t per_set = sizeof(float) * (size_t)k * k;
+  long long chunk = (long long)(chunk_bytes() / per_set);
+  if (chunk < 1) chunk = 1;
+  if (chunk > nsets) chunk = nsets;
+  rc = grow(g.blocks, g.blocks_bytes, per_set * (size_t)chunk);
+  if (rc) return rc;
+  void* gp = g.gerr;
+  size_t gb = g.gerr_count * sizeof(int);
+  rc = grow(gp, gb, sizeof(int) * (size_t)chunk);
+  if (rc) return rc;
+  g.gerr = (int*)gp;
+  g.gerr_count = gb / sizeof(int);
+  rc = ensure_status(g, st);
+  if (rc) return rc;
+  const bool all = eig || det;
+  MatrixF32 M{(const float*)g.blocks, (long long)k, k, (long long)k * k};
+  for (long long s0 = 0; s0 < nsets; s0 += chunk) {
+    const long long cnt = nsets - s0 < chunk ? nsets - s0 : chunk;
+    const int* ci = idx + s0 * k;
+    GCU(cudaMemsetAsync(g.gerr, 0, sizeof(int) * (size_t)cnt, st));
+    rc = launch_gram(prep, m, n, ci, cnt, k, (float*)g.blocks, g.gerr, g.status, st);
+    if (rc) return rc;
+    SetOutputs out{lmin ? lmin + s0 : nullptr, lmax ? lmax + s0 : nullptr,
+                   delta ? delta + s0 : nullptr, err ? err + s0 : nullptr,
+                   eig ? eig + s0 * k : nullptr, det ? det + s0 : nullptr};
+    rc = api_solve_uniform(M, ci, cnt, k, form, out, st);
+    if (rc) return rc;
+    const long long gblk = (cnt + 255) / 256;
+    k_gram_fixup<<<(unsigned)(gblk < 1024 ? gblk : 1024), 256, 0, st>>>(g.gerr, cnt, out, k, all);
+    GCU(cudaGetLastError());
+  }
+  return check_status(g, st);
+}
+
+}  // extern "C"

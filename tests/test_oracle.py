@@ -162,3 +162,16 @@ def test_sturm_decoupled_and_degenerate():
     ev = np.linalg.eigvalsh(T)
     np.testing.assert_allclose(O.bisect_all(a, b2), ev, rtol=0, atol=1e-13 * 1e20)
     assert O.sturm_count(a, b2, 1e19) == 100
+
+
+def test_dsg_b_matches_blas_and_offset():
+    """DSG_B restatement (ParaLanczos.cu:364-382): Gram of frame columns S,
+    frame row-major M x N, column offset applied to every index."""
+    rng = np.random.default_rng(0)
+    F = rng.standard_normal((37, 50))
+    S = np.array([3, 7, 1, 49], dtype=np.int32)
+    G = O.dsg_b(F, S)
+    assert np.allclose(G, F[:, S].T @ F[:, S], rtol=0, atol=1e-12)
+    assert np.array_equal(G, G.T)
+    G1 = O.dsg_b(F, S[:3], off=1)
+    assert np.allclose(G1, F[:, S[:3] + 1].T @ F[:, S[:3] + 1], rtol=0, atol=1e-12)
