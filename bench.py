@@ -2,6 +2,11 @@
 """Benchmark: subset eigen-solves/s at k=64 (batched vs plain), one JSON line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c2|c3|c4|c5]
+
+The default workload (c2) is the headline configuration described below;
+c3 (uneven k in one launch), c4 (on-the-fly Gram) and c5 (serving) print
+their own JSON line with the same keys (see bench_extra.py).
 
 Workload (the configuration the headline metric is quoted on): Phi 1024x4096
 with i.i.d. N(0, 1/1024) entries (seeded, generated on the GPU in FP64),
@@ -369,7 +374,13 @@ def main() -> int:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU-baseline work")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"])
+    ap.add_argument("--rates", default="", help="c5: comma-separated request rates (1/s) to sweep")
+    ap.add_argument("--requests", type=int, default=0, help="c5: requests per rate")
     args = ap.parse_args()
+    if args.workload != "c2":
+        import bench_extra
+        return bench_extra.run(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -140,6 +140,40 @@ int pl_solve_gram(const void *prep, int m, int n, const int *idx, long long nset
                   int form, double *lmin, double *lmax, double *delta, int *err, double *eig,
                   double *det, void *stream);
 
+/* ---- serving: continuous batching of requests ----------------------------
+ * No counterpart in the reference (each calculate_subeigs* call is one
+ * synchronous batch on one matrix, ParaLanczos.cu:1725-1863).  A server keeps
+ * matrices resident and solves requests (matrix, k, nsets index sets) as they
+ * arrive: a scheduler thread admits queued requests in arrival order while
+ * their indices fit `budget_bytes` of HBM, and runs the admitted work in
+ * waves of about PL_SERVE_WAVE_MS (default 20) ms of GPU work -- sets of any
+ * matrix and k, binned by k on the device; large requests are split over
+ * waves and small ones go first -- with up to `max_waves` waves in flight on
+ * their own streams.  Extremes only (lambda_min, lambda_max, delta_k, err).
+ * Host buffers; thread-safe.                                                 */
+/* `host_pool_bytes` of pinned memory stage submitted indices and results.    */
+int pl_serve_create(long long budget_bytes, long long host_pool_bytes, int max_waves, void **server);
+/* Register a device-resident symmetric FP32 matrix (kept by reference: it must
+ * stay allocated and unchanged while the server lives).                      */
+int pl_serve_add_matrix(void *server, const float *A, int n, long long lda, int *matrix_id);
+/* Queue a request: idx = nsets*k host indices (copied).  PL_EBUSY: the pinned
+ * pool is full (retry after collecting results); PL_EINVAL: bad arguments or a
+ * request larger than the budget.                                            */
+int pl_serve_submit(void *server, int matrix_id, const int *idx, long long nsets, int k,
+                    long long *request_id);
+/* Wait up to timeout_s for a request; on PL_OK copies its results (each
+ * output nullable, nsets entries) and the submit-to-completion latency, and
+ * forgets the request.  PL_ETIMEDOUT: not finished yet (still queued).       */
+int pl_serve_wait(void *server, long long request_id, double timeout_s, double *lmin, double *lmax,
+                  double *delta, int *err, double *latency_s);
+/* out[0..11]: completed requests, sets solved, p50, p99, mean and max latency
+ * (s), busy span first admission .. last completion (s), peak and total arena
+ * bytes, waves launched, most waves in flight at once, requests queued.      */
+int pl_serve_stats(void *server, double *out, int nout);
+int pl_serve_reset_stats(void *server);
+/* Stops the scheduler (in-flight waves finish first) and frees everything.  */
+int pl_serve_destroy(void *server);
+
 /* ---- ParaLanczos.h drop-ins with a status return ------------------------ */
 /* Host pointers, FP64 matrix, all eigenvalues out; semantics of the named
  * reference routine (validation messages, output layout).  PL_STRICT=0 in the

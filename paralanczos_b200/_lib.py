@@ -46,6 +46,13 @@ SIGNATURES = {
     "pl_gram_prepare": (_i, [_vp, _ll, _i, _i, _vp, _vp]),
     "pl_gram_blocks": (_i, [_vp, _i, _i, _vp, _ll, _i, _vp, _vp, _vp]),
     "pl_solve_gram": (_i, [_vp, _i, _i, _vp, _ll, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "pl_serve_create": (_i, [_ll, _ll, _i, C.POINTER(_vp)]),
+    "pl_serve_add_matrix": (_i, [_vp, _vp, _i, _ll, C.POINTER(_i)]),
+    "pl_serve_submit": (_i, [_vp, _i, _vp, _ll, _i, C.POINTER(_ll)]),
+    "pl_serve_wait": (_i, [_vp, _ll, _d, _vp, _vp, _vp, _vp, C.POINTER(_d)]),
+    "pl_serve_stats": (_i, [_vp, C.POINTER(_d), _i]),
+    "pl_serve_reset_stats": (_i, [_vp]),
+    "pl_serve_destroy": (_i, [_vp]),
 }
 
 _lib = None

@@ -257,3 +257,87 @@ class GramFrame:
                                   FORMS[form], p("lmin"), p("lmax"), p("delta"), p("err"), p("eig"),
                                   p("det"), st.cuda_stream), "pl_solve_gram")
         return out
+
+
+# --------------------------------------------------------------------------- serving
+
+SERVE_STATS = ("completed", "sets", "p50_s", "p99_s", "mean_s", "max_s", "busy_s", "arena_peak",
+               "arena_bytes", "waves", "waves_inflight_max", "queued")
+
+
+class Server:
+    """Continuous-batching server over device-resident matrices (pl_serve_*).
+
+    ``submit`` queues a request and returns its id (raises PLError with status
+    PL_EBUSY when the pinned pool is full); ``wait`` returns its results as a
+    dict of numpy arrays plus ``latency_s`` (submit to completion)."""
+
+    def __init__(self, budget_bytes: int = 1 << 30, host_pool_bytes: int = 1 << 30, max_waves: int = 3):
+        self._h = C.c_void_p()
+        self._mats = []   # keep the registered tensors alive
+        check(lib().pl_serve_create(int(budget_bytes), int(host_pool_bytes), int(max_waves),
+                                    C.byref(self._h)), "pl_serve_create")
+
+    def add_matrix(self, A) -> int:
+        import torch
+        if A.dtype != torch.float32 or not A.is_cuda or A.dim() != 2 or A.stride(1) != 1:
+            raise TypeError("A must be a row-major 2-D float32 CUDA tensor")
+        torch.cuda.current_stream(A.device).synchronize()
+        mid = C.c_int(-1)
+        check(lib().pl_serve_add_matrix(self._h, A.data_ptr(), A.shape[0], A.stride(0), C.byref(mid)),
+              "pl_serve_add_matrix")
+        self._mats.append(A)
+        return mid.value
+
+    def submit(self, matrix_id: int, idx, k: int) -> int:
+        idx = _need(np.ascontiguousarray(idx, dtype=np.int32).reshape(-1), np.int32, "idx")
+        rid = C.c_longlong(0)
+        check(lib().pl_serve_submit(self._h, int(matrix_id), idx.ctypes.data, len(idx) // int(k), int(k),
+                                    C.byref(rid)), "pl_serve_submit")
+        return rid.value
+
+    def try_submit(self, matrix_id: int, idx, k: int):
+        """Like submit, but returns None instead of raising when the pool is full."""
+        idx = _need(np.ascontiguousarray(idx, dtype=np.int32).reshape(-1), np.int32, "idx")
+        rid = C.c_longlong(0)
+        rc = lib().pl_serve_submit(self._h, int(matrix_id), idx.ctypes.data, len(idx) // int(k), int(k),
+                                   C.byref(rid))
+        if rc == _lib.PL_EBUSY:
+            return None
+        check(rc, "pl_serve_submit")
+        return rid.value
+
+    def wait(self, request_id: int, nsets: int, timeout_s: float = 60.0):
+        out = dict(lmin=np.empty(nsets), lmax=np.empty(nsets), delta=np.empty(nsets),
+                   err=np.empty(nsets, dtype=np.int32))
+        lat = C.c_double(0.0)
+        check(lib().pl_serve_wait(self._h, int(request_id), float(timeout_s), out["lmin"].ctypes.data,
+                                  out["lmax"].ctypes.data, out["delta"].ctypes.data, out["err"].ctypes.data,
+                                  C.byref(lat)), "pl_serve_wait")
+        out["latency_s"] = lat.value
+        return out
+
+    def stats(self) -> dict:
+        buf = (C.c_double * len(SERVE_STATS))()
+        check(lib().pl_serve_stats(self._h, buf, len(SERVE_STATS)), "pl_serve_stats")
+        return dict(zip(SERVE_STATS, list(buf)))
+
+    def reset_stats(self) -> None:
+        check(lib().pl_serve_reset_stats(self._h), "pl_serve_reset_stats")
+
+    def close(self) -> None:
+        if self._h:
+            check(lib().pl_serve_destroy(self._h), "pl_serve_destroy")
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -380,6 +380,69 @@ int solve_uniform(const MatrixF32& M, const int* idx, long long nsets, int k, in
   return PL_OK;
 }
 
+// Per-bin queue-scratch layout of one binned launch: region b at off[b].
+size_t binned_qscratch(int form, bool all, size_t off[kNumBins]) {
+  size_t total = 0;
+  for (int b = 0; b < kNumBins; ++b) {
+    off[b] = total;
+    const bool plain_bin = form == PL_FORM_PLAIN && kBinK[b] <= 128;
+    const size_t need = plain_bin ? 0 : chosen_for(b, all).scratch[all ? 1 : 0]();
+    total += (need + 255) & ~(size_t)255;
+  }
+  return total;
+}
+
+void binned_fns(int form, bool all, LaunchFn fns[kNumBins]) {
+  for (int b = 0; b < kNumBins; ++b)
+    fns[b] = (form == PL_FORM_PLAIN && kBinK[b] <= 128) ? plain_fn(kBinK[b], all)
+                                                        : chosen_for(b, all).fn[all ? 1 : 0];
+}
+
+// The binned sequence on stream cs: count sets per k bin, scan, scatter the
+// set ids into per-bin queues (perm), flag bad k, then one persistent launch
+// per bin on the forked side streams (largest k first, so the small-k kernels
+// fill the tail), joined back into cs.  hdr: 48 ints (counts, starts, cursor)
+// followed by nsets ints of perm.
+cudaError_t enqueue_binned(const MatrixF32& M, const int* idx, const long long* offsets,
+                           long long nsets, const SetOutputs& out, const LaunchFn fns[kNumBins],
+                           int* hdr, char* qscratch, const size_t qoff[kNumBins], cudaStream_t cs,
+                           const cudaStream_t side[kNumBins], cudaEvent_t fork,
+                           const cudaEvent_t join[kNumBins]) {
+  const int nb = kNumBins;
+  int* counts = hdr;
+  int* starts = hdr + 16;
+  int* cursor = hdr + 32;
+  int* perm = hdr + 48;
+  BinTable bt;
+  bt.nb = nb;
+  for (int b = 0; b < nb; ++b) bt.kmax[b] = kBinK[b];
+  cudaError_t e = cudaSuccess;
+  auto note = [&](cudaError_t x) {
+    if (e == cudaSuccess && x != cudaSuccess) e = x;
+  };
+  note(cudaMemsetAsync(counts, 0, sizeof(int) * 16, cs));
+  const int tb = 256;
+  const long long g = (nsets + tb - 1) / tb;
+  const unsigned grid = (unsigned)(g < 4096 ? (g > 0 ? g : 1) : 4096);
+  k_bin_count<<<grid, tb, 0, cs>>>(offsets, nsets, bt, counts);
+  note(cudaGetLastError());
+  k_bin_scan<<<1, 32, 0, cs>>>(counts, nb, starts, cursor);
+  note(cudaGetLastError());
+  k_bin_scatter<<<grid, tb, 0, cs>>>(offsets, nsets, bt, starts, cursor, perm);
+  note(cudaGetLastError());
+  k_mark_bad_k<<<64, 256, 0, cs>>>(perm, starts + nb, counts + nb, offsets, out);
+  note(cudaGetLastError());
+  note(cudaEventRecord(fork, cs));
+  for (int b = nb - 1; b >= 0 && e == cudaSuccess; --b) {
+    note(cudaStreamWaitEvent(side[b], fork, 0));
+    SetSource src{idx, offsets, 0, perm, starts + b, counts + b, 0};
+    note(fns[b](M, src, out, -1, qscratch + qoff[b], side[b], false));
+    note(cudaEventRecord(join[b], side[b]));
+    note(cudaStreamWaitEvent(cs, join[b], 0));
+  }
+  return e;
+}
+
 // Uneven k (CSR): device binning, then one persistent launch per non-empty
 // bin on forked streams, all captured into one CUDA graph (cached by the call
 // signature) and launched as one unit.
@@ -389,20 +452,12 @@ int solve_csr(const MatrixF32& M, const int* idx, const long long* offsets, long
   DevState& d = state();
   int rc = ensure_streams(d);
   if (rc) return rc;
-  const int nb = kNumBins;
-  const size_t hdr = 3 * 16;  // counts / starts / cursor, 16 ints each
-  rc = ensure(d.bins, sizeof(int) * (hdr + (size_t)nsets));
+  rc = ensure(d.bins, sizeof(int) * (48 + (size_t)nsets));
   if (rc) return rc;
   // every bin gets its own scratch region: the bins run concurrently
-  size_t large_off[kNumBins] = {0};
-  size_t large_total = 0;
-  for (int b = 0; b < nb; ++b) {
-    large_off[b] = large_total;
-    const bool plain_bin = form == PL_FORM_PLAIN && kBinK[b] <= 128;
-    const size_t need = plain_bin ? 0 : chosen_for(b, all).scratch[all ? 1 : 0]();
-    large_total += (need + 255) & ~(size_t)255;
-  }
-  rc = ensure(d.large, large_total > 0 ? large_total : 256);
+  size_t qoff[kNumBins];
+  const size_t qtotal = binned_qscratch(form, all, qoff);
+  rc = ensure(d.large, qtotal > 0 ? qtotal : 256);
   if (rc) return rc;
   char keybuf[512];
   snprintf(keybuf, sizeof keybuf, "%p|%d|%lld|%p|%p|%lld|%d|%p|%p|%p|%p|%p|%p|%d%d%d%d%d%d%d",
@@ -413,52 +468,22 @@ int solve_csr(const MatrixF32& M, const int* idx, const long long* offsets, long
   const std::string key(keybuf);
   auto it = d.graphs.find(key);
   if (it == d.graphs.end()) {
-    int* counts = (int*)d.bins.p;
-    int* starts = counts + 16;
-    int* cursor = counts + 32;
-    int* perm = counts + 48;
-    BinTable bt;
-    bt.nb = nb;
-    for (int b = 0; b < nb; ++b) bt.kmax[b] = kBinK[b];
     LaunchFn fns[kNumBins];
-    for (int b = 0; b < nb; ++b) {
-      fns[b] = (form == PL_FORM_PLAIN && kBinK[b] <= 128) ? plain_fn(kBinK[b], all)
-                                                          : chosen_for(b, all).fn[all ? 1 : 0];
-      // load every kernel before the capture: nothing that may load a module
-      // or set a function attribute runs while the stream is capturing
-      PL_CU(fns[b](M, SetSource{}, out, 0, nullptr, d.side[b], true));
-    }
+    binned_fns(form, all, fns);
+    // load every kernel before the capture: nothing that may load a module
+    // or set a function attribute runs while the stream is capturing
+    for (int b = 0; b < kNumBins; ++b) PL_CU(fns[b](M, SetSource{}, out, 0, nullptr, d.side[b], true));
     cudaStream_t cs = d.cap;  // graphs do not depend on the stream they were captured on
     PL_CU(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = cudaSuccess;
-    auto note = [&](cudaError_t x) {
-      if (e == cudaSuccess && x != cudaSuccess) e = x;
-    };
-    note(cudaMemsetAsync(counts, 0, sizeof(int) * 16, cs));
-    const int tb = 256;
-    const long long g = (nsets + tb - 1) / tb;
-    const unsigned grid = (unsigned)(g < 4096 ? (g > 0 ? g : 1) : 4096);
-    k_bin_count<<<grid, tb, 0, cs>>>(offsets, nsets, bt, counts);
-    note(cudaGetLastError());
-    k_bin_scan<<<1, 32, 0, cs>>>(counts, nb, starts, cursor);
-    note(cudaGetLastError());
-    k_bin_scatter<<<grid, tb, 0, cs>>>(offsets, nsets, bt, starts, cursor, perm);
-    note(cudaGetLastError());
-    k_mark_bad_k<<<64, 256, 0, cs>>>(perm, starts + nb, counts + nb, offsets, out);
-    note(cudaGetLastError());
-    note(cudaEventRecord(d.ev_fork, cs));
-    // largest-k bins first so the small-k kernels fill the tail
-    for (int b = nb - 1; b >= 0 && e == cudaSuccess; --b) {
-      note(cudaStreamWaitEvent(d.side[b], d.ev_fork, 0));
-      SetSource src{idx, offsets, 0, perm, starts + b, counts + b, 0};
-      note(fns[b](M, src, out, -1, (char*)d.large.p + large_off[b], d.side[b], false));
-      note(cudaEventRecord(d.ev_join[b], d.side[b]));
-      note(cudaStreamWaitEvent(cs, d.ev_join[b], 0));
-    }
+    cudaError_t e = enqueue_binned(M, idx, offsets, nsets, out, fns, (int*)d.bins.p, (char*)d.large.p,
+                                   qoff, cs, d.side, d.ev_fork, d.ev_join);
     cudaGraph_t graph = nullptr;
-    note(cudaStreamEndCapture(cs, &graph));  // always ends the capture
+    {
+      cudaError_t e2 = cudaStreamEndCapture(cs, &graph);  // always ends the capture
+      if (e == cudaSuccess) e = e2;
+    }
     cudaGraphExec_t exec = nullptr;
-    if (e == cudaSuccess) note(cudaGraphInstantiate(&exec, graph, 0));
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
     if (graph) cudaGraphDestroy(graph);
     if (e != cudaSuccess) {
       if (exec) cudaGraphExecDestroy(exec);
@@ -518,6 +543,25 @@ int api_solve_uniform(const MatrixF32& M, const int* idx, long long nsets, int k
   return solve_uniform(M, idx, nsets, k, form, out, st);
 }
 std::mutex& api_mutex() { return g_mu; }
+int api_num_bins() { return kNumBins; }
+size_t api_binned_scratch(long long nsets, int form, bool all) {
+  size_t qoff[kNumBins];
+  return align256(sizeof(int) * (48 + (size_t)nsets)) + binned_qscratch(form, all, qoff);
+}
+int api_launch_binned(const MatrixF32& M, const int* idx, const long long* offsets, long long nsets,
+                      int form, const SetOutputs& out, void* scratch, cudaStream_t st,
+                      const cudaStream_t* side, cudaEvent_t fork, const cudaEvent_t* join) {
+  const bool all = out.eig || out.det;
+  size_t qoff[kNumBins];
+  binned_qscratch(form, all, qoff);
+  LaunchFn fns[kNumBins];
+  binned_fns(form, all, fns);
+  char* base = (char*)scratch;
+  int* hdr = (int*)base;
+  char* q = base + align256(sizeof(int) * (48 + (size_t)nsets));
+  PL_CU(enqueue_binned(M, idx, offsets, nsets, out, fns, hdr, q, qoff, st, side, fork, join));
+  return PL_OK;
+}
 void api_note_cuda(cudaError_t e) { g_last_cuda = (int)e; }
 int api_device_sms() { return device_sms(); }
 }  // namespace pl

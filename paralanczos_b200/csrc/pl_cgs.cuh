@@ -39,11 +39,12 @@ __device__ __forceinline__ void cgs_solve_set(const MatrixF32& M, const int* __r
   constexpr int NW = NT > 32 ? NT / 32 : 1;
   const int t = g.t;
 
+  const SetMatrix SM = set_matrix(M, set);
   bool bad = false;
   for (int c = t; c < k; c += NT) {
-    const int v = set_index(M, S, c);
-    bad |= (v < 0) | (v >= M.n);
-    sm.idx[c] = (v >= 0 && v < M.n) ? v : 0;
+    const int v = SM.index(S, c);
+    bad |= (v < 0) | (v >= SM.n);
+    sm.idx[c] = (v >= 0 && v < SM.n) ? v : 0;
   }
   if (group_any<NT, NW>(bad, g, sm.red[3])) {
     if (t == 0) write_failed(out, set, off, ALL ? k : 0, SET_BAD_INDEX);
@@ -55,7 +56,7 @@ __device__ __forceinline__ void cgs_solve_set(const MatrixF32& M, const int* __r
   // gather A[S,S] (column c, row i) into As; Frobenius norm
   double fro = 0.0;
   for (int c = 0; c < k; ++c) {
-    const float* __restrict__ arow = set_base(M, set) + (size_t)sm.idx[c] * (size_t)M.lda;  // row S_c = column S_c
+    const float* __restrict__ arow = SM.A + (size_t)sm.idx[c] * (size_t)SM.lda;  // row S_c = column S_c
     for (int i = t; i < k; i += NT) {
       const float a = __ldg(arow + sm.idx[i]);
       As[(size_t)c * lda + i] = a;

@@ -90,14 +90,15 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
   const unsigned rmask = (TPR == 32) ? 0xffffffffu : (((1u << TPR) - 1u) << ((t & 31) / TPR * TPR));
 
   // ---- indices (every CTA keeps the full set), validation -------------------
+  const SetMatrix SM = set_matrix(M, set);
   bool bad = false;
   for (int c = t; c < KB; c += NTC) {
     int v = 0;
     if (c < k) {
-      v = set_index(M, S, c);
-      bad |= (v < 0) | (v >= M.n);
+      v = SM.index(S, c);
+      bad |= (v < 0) | (v >= SM.n);
     }
-    sm.idx[c] = (c < k && v >= 0 && v < M.n) ? v : 0;
+    sm.idx[c] = (c < k && v >= 0 && v < SM.n) ? v : 0;
   }
   const double badsum = cluster_sum<KB, CS, NTC>(__any_sync(0xffffffffu, bad) ? 1.0 : 0.0, sm, 3, cl, rank);
   if (badsum != 0.0) {
@@ -112,7 +113,7 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
   double fro = 0.0;
   {
     const bool rv = r < k;
-    const float* __restrict__ arow = set_base(M, set) + (size_t)sm.idx[r] * (size_t)M.lda;
+    const float* __restrict__ arow = SM.A + (size_t)sm.idx[r] * (size_t)SM.lda;
 #pragma unroll
     for (int ch = 0; ch < NCH; ++ch) {
       float e[4];

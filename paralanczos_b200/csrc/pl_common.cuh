@@ -38,6 +38,14 @@ struct SetOutputs {
   double* det;    // product of eigenvalues (nullable)
 };
 
+// One device-resident matrix of a table (serving: sets of one launch may
+// name different matrices).
+struct MatrixRef {
+  const float* A;
+  long long lda;
+  int n;
+};
+
 struct MatrixF32 {
   const float* A;  // symmetric, row-major
   long long lda;
@@ -46,16 +54,29 @@ struct MatrixF32 {
   // A + set * set_stride, indexed locally 0..k-1 (the on-the-fly Gram form);
   // n is then the block dimension.
   long long set_stride = 0;
+  // non-null: set s reads matrix mats[mat_id[s]] instead of A / lda / n.
+  const MatrixRef* mats = nullptr;
+  const int* mat_id = nullptr;
 };
 
-// Row/column of the matrix the engines read for position c of the set.
-__device__ __forceinline__ int set_index(const MatrixF32& M, const int* __restrict__ S, int c) {
-  return M.set_stride ? c : __ldg(S + c);
-}
+// The matrix one set reads, resolved once at the start of its solve.
+struct SetMatrix {
+  const float* A;
+  long long lda;
+  int n;
+  bool local;  // indices are block-local 0..k-1 (pre-formed block)
+  __device__ __forceinline__ int index(const int* __restrict__ S, int c) const {
+    return local ? c : __ldg(S + c);
+  }
+};
 
-// Base of the matrix the set's rows are read from.
-__device__ __forceinline__ const float* set_base(const MatrixF32& M, long long set) {
-  return M.set_stride ? M.A + set * M.set_stride : M.A;
+__device__ __forceinline__ SetMatrix set_matrix(const MatrixF32& M, long long set) {
+  if (M.mat_id) {
+    const MatrixRef r = M.mats[__ldg(M.mat_id + set)];
+    return SetMatrix{r.A, r.lda, r.n, false};
+  }
+  if (M.set_stride) return SetMatrix{M.A + set * M.set_stride, M.lda, M.n, true};
+  return SetMatrix{M.A, M.lda, M.n, false};
 }
 
 __device__ __forceinline__ long long item_count(const SetSource& src) {

@@ -186,14 +186,15 @@ __device__ __forceinline__ int solve_set(const MatrixF32& M, const int* __restri
   const bool lead = (t % TPR) == 0;  // one thread per row contributes to row reductions
 
   // ---- indices -> shared memory, validation --------------------------------
+  const SetMatrix SM = set_matrix(M, set);
   bool bad = false;
   for (int c = t; c < KB; c += NT) {
     int v = 0;
     if (c < k) {
-      v = set_index(M, S, c);
-      bad |= (v < 0) | (v >= M.n);
+      v = SM.index(S, c);
+      bad |= (v < 0) | (v >= SM.n);
     }
-    sm.idx[c] = (c < k && v >= 0 && v < M.n) ? v : 0;
+    sm.idx[c] = (c < k && v >= 0 && v < SM.n) ? v : 0;
   }
   if (group_any<NT, NW>(bad, g, sm.red[3])) {
     if (t == 0) write_failed(out, set, off, ALL ? k : 0, SET_BAD_INDEX);
@@ -213,7 +214,7 @@ __device__ __forceinline__ int solve_set(const MatrixF32& M, const int* __restri
     const int r = rs + q * C::RSLOTS;
     rowid[q] = r;
     const bool rv = r < k;
-    const float* __restrict__ arow = set_base(M, set) + (size_t)sm.idx[r] * (size_t)M.lda;
+    const float* __restrict__ arow = SM.A + (size_t)sm.idx[r] * (size_t)SM.lda;
 #pragma unroll
     for (int cc = 0; cc < CPT; cc += 2) {
       const int c = c0 + cc;

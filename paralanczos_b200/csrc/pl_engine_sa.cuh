@@ -49,14 +49,15 @@ __device__ __forceinline__ int solve_set_sa(const MatrixF32& M, const int* __res
   const int t = g.t;
 
   // ---- indices -> shared memory, validation ---------------------------------
+  const SetMatrix SM = set_matrix(M, set);
   bool bad = false;
   for (int c = t; c < KB; c += NT) {
     int v = 0;
     if (c < k) {
-      v = set_index(M, S, c);
-      bad |= (v < 0) | (v >= M.n);
+      v = SM.index(S, c);
+      bad |= (v < 0) | (v >= SM.n);
     }
-    sm.idx[c] = (c < k && v >= 0 && v < M.n) ? v : 0;
+    sm.idx[c] = (c < k && v >= 0 && v < SM.n) ? v : 0;
   }
   if (group_any<NT, NW>(bad, g, sm.red[3])) {
     if (t == 0) write_failed(out, set, off, ALL ? k : 0, SET_BAD_INDEX);
@@ -73,7 +74,7 @@ __device__ __forceinline__ int solve_set_sa(const MatrixF32& M, const int* __res
   for (int q = 0; q < RPT; ++q) {
     const int r = t + q * NT;
     const bool rv = r < k;
-    const float* __restrict__ arow = set_base(M, set) + (size_t)sm.idx[r] * (size_t)M.lda;
+    const float* __restrict__ arow = SM.A + (size_t)sm.idx[r] * (size_t)SM.lda;
 #pragma unroll
     for (int ch = 0; ch < NCH; ++ch) {
       float e[4];

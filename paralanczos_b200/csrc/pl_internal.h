@@ -13,6 +13,21 @@ namespace pl {
 int api_solve_uniform(const MatrixF32& M, const int* idx, long long nsets, int k, int form,
                       const SetOutputs& out, cudaStream_t st);
 
+// Number of k bins of the batched kernels.
+int api_num_bins();
+
+// Device scratch (bytes) of one api_launch_binned call over nsets sets.
+size_t api_binned_scratch(long long nsets, int form, bool all);
+
+// Binned CSR launch enqueued directly on `st` (no graph capture): device-side
+// counting sort of the sets by k bin, then one persistent kernel per bin on
+// the side streams side[0..nbins) (fork/join through the given events).
+// `scratch` holds api_binned_scratch(nsets, ...) bytes used by this launch
+// alone until it completes.
+int api_launch_binned(const MatrixF32& M, const int* idx, const long long* offsets, long long nsets,
+                      int form, const SetOutputs& out, void* scratch, cudaStream_t st,
+                      const cudaStream_t* side, cudaEvent_t fork, const cudaEvent_t* join);
+
 // Serialises calls that touch the per-device cached state.
 std::mutex& api_mutex();
 
