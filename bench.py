@@ -317,7 +317,7 @@ def run_ours(args):
     peak_fp32 = api.fp32_peak()
     peaks, peak_src = measured_peaks()
     achieved = flops_per_set(K) * NSETS / (my_ms * 1e-3) / 1e12
-    traffic = profile_traffic("k_reg_solve_k64_c2.md")
+    traffic = profile_traffic("k_sa_solve_k64_c2.md")
     gather_gbs = gather_bytes_per_set(K) * NSETS / (my_ms * 1e-3) / 1e9
 
     cpu = None

@@ -304,6 +304,7 @@ def run_c4(args):
                                   "traffic": None, "kernel": "Lanczos k=128 on the formed blocks "
                                   "(the dominant kernel: step time minus the Gram kernel's)"},
                      "roofline_gram": {"bound": "tensor", "achieved": tensor_tf,
+                                       "traffic_8192_sets": B.profile_traffic("k_gram_c4.md"),
                                        "peak": peaks.get("bf16_tflops"), "unit": "TFLOP/s",
                                        "frac": tensor_tf / peaks.get("bf16_tflops"), "peak_source": src,
                                        "useful_tflops": useful / (r["gram_ms"] * 1e-3) / 1e12,

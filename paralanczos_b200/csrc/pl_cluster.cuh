@@ -15,9 +15,12 @@
 // w~ = y - alpha v_j - beta_j v_{j-1} locally), one carries the rows of w with
 // the ||w||^2 partials.
 //
-// Thread mapping inside a CTA: NTC threads, TPR = NTC / R threads per row, a
-// thread owns CPT = KB / TPR consecutive columns of its row; row partial sums
-// are combined with xor-shuffles over the TPR lanes (TPR divides 32).
+// Thread mapping inside a CTA: NTC threads, TPR = NTC / R threads per row;
+// thread g = t % TPR of a row owns the float4 column chunks g, g + TPR,
+// g + 2 TPR, ... (CPT = KB / TPR columns), so the TPR threads of a row read
+// adjacent 16-byte chunks of a broadcast vector: conflict-free shared-memory
+// loads.  Row partial sums are combined with xor-shuffles over the TPR lanes
+// (TPR divides 32).
 #pragma once
 #include <cooperative_groups.h>
 
@@ -85,8 +88,8 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
   const int t = threadIdx.x;
   const int lr = t / TPR;              // local row
   const int r = rank * R + lr;         // global row
-  const int c0 = (t % TPR) * CPT;      // first owned column
-  const bool lead = (t % TPR) == 0;
+  const int g0 = t % TPR;              // owned chunks g0 + TPR * ch
+  const bool lead = g0 == 0;
   const unsigned rmask = (TPR == 32) ? 0xffffffffu : (((1u << TPR) - 1u) << ((t & 31) / TPR * TPR));
 
   // ---- indices (every CTA keeps the full set), validation -------------------
@@ -119,12 +122,12 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
       float e[4];
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        const int c = c0 + 4 * ch + u;
+        const int c = 4 * (g0 + TPR * ch) + u;
         e[u] = (rv && c < k) ? __ldg(arow + sm.idx[c]) : 0.f;
         fro += (double)e[u] * (double)e[u];
       }
       my[ch * NTC] = make_float4(e[0], e[1], e[2], e[3]);
-      const int c = c0 + 4 * ch;
+      const int c = 4 * (g0 + TPR * ch);
       Pr[2 * ch] = make_float2((rv && c == r) ? 1.f : 0.f, (rv && c + 1 == r) ? 1.f : 0.f);
       Pr[2 * ch + 1] = make_float2((rv && c + 2 == r) ? 1.f : 0.f, (rv && c + 3 == r) ? 1.f : 0.f);
     }
@@ -154,7 +157,7 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
     const float2 nc = make_float2(cq, cq);
 #pragma unroll
     for (int ch = 0; ch < NCH; ++ch) {
-      const float4 b4 = *reinterpret_cast<const float4*>(&sm.vb[cur][c0 + 4 * ch]);
+      const float4 b4 = *reinterpret_cast<const float4*>(&sm.vb[cur][4 * (g0 + TPR * ch)]);
       const float4 a4 = my[ch * NTC];
       const float2 b01 = make_float2(b4.x, b4.y), b23 = make_float2(b4.z, b4.w);
       Pr[2 * ch] = __ffma2_rn(nc, b01, Pr[2 * ch]);
@@ -182,7 +185,7 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
     float2 wa = make_float2(0.f, 0.f), wc = make_float2(0.f, 0.f);
 #pragma unroll
     for (int ch = 0; ch < NCH; ++ch) {
-      const float4 x4 = *reinterpret_cast<const float4*>(&sm.wb[c0 + 4 * ch]);
+      const float4 x4 = *reinterpret_cast<const float4*>(&sm.wb[4 * (g0 + TPR * ch)]);
       wa = __ffma2_rn(Pr[2 * ch], make_float2(x4.x, x4.y), wa);
       wc = __ffma2_rn(Pr[2 * ch + 1], make_float2(x4.z, x4.w), wc);
     }
@@ -214,12 +217,15 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
       // (cluster-wide argmax, ties to the smaller row), published into vb[nxt].
       status |= SET_BREAKDOWN;
       unsigned long long kk = 0ull;
-      if (r < k && r >= c0 && r < c0 + CPT) {
+      if (r < k && ((r >> 2) - g0) % TPR == 0) {  // this thread owns column r
         float d = 0.f;
 #pragma unroll
-        for (int c = 0; c < CPT; c += 2) {
-          if (c0 + c == r) d = Pr[c / 2].x;
-          if (c0 + c + 1 == r) d = Pr[c / 2].y;
+        for (int ch = 0; ch < NCH; ++ch) {
+          const int c = 4 * (g0 + TPR * ch);
+          if (c == r) d = Pr[2 * ch].x;
+          if (c + 1 == r) d = Pr[2 * ch].y;
+          if (c + 2 == r) d = Pr[2 * ch + 1].x;
+          if (c + 3 == r) d = Pr[2 * ch + 1].y;
         }
         d = fmaxf(d, 0.f);
         kk = ((unsigned long long)__float_as_uint(d) << 32) | (unsigned)(0x7fffffff - r);
@@ -249,9 +255,12 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
         for (int q = 0; q < CS; ++q) {
           float* dst = cl.map_shared_rank(&sm, (unsigned)q)->vb[nxt];
 #pragma unroll
-          for (int c = 0; c < CPT; c += 2) {
-            dst[c0 + c] = Pr[c / 2].x;
-            dst[c0 + c + 1] = Pr[c / 2].y;
+          for (int ch = 0; ch < NCH; ++ch) {
+            const int c = 4 * (g0 + TPR * ch);
+            dst[c] = Pr[2 * ch].x;
+            dst[c + 1] = Pr[2 * ch].y;
+            dst[c + 2] = Pr[2 * ch + 1].x;
+            dst[c + 3] = Pr[2 * ch + 1].y;
           }
         }
       }

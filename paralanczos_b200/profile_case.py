@@ -1,0 +1,75 @@
+"""Small, self-contained cases of the library's kernels for profiling.
+
+Each case builds its inputs on the GPU, runs the kernel once to warm up
+(module load, scratch allocation) and then `--launches` more times, so a
+profiler can skip the first launch and capture the next ones:
+
+    python -m paralanczos_b200.profile_case --case k64 [--nsets 200000]
+    ncu --set full --clock-control none -k regex:k_sa_solve -s 1 -c 1 \\
+        python -m paralanczos_b200.profile_case --case k64
+
+Cases:
+  k64      batched form, k = 64, A = Phi^T Phi (Phi 1024 x 4096 N(0, 1/1024)),
+           sets from the counter-based generator (seed 1); the tuned variant.
+  plain64  the same sets through the one-set-per-block form.
+  k128     batched form, k = 128 on the same matrix.
+  k256     batched form, k = 256 (thread-block-cluster engine).
+  gram     on-the-fly Gram blocks, Phi 2048 x 16384 N(0, 1/2048), k = 128.
+  uneven   binned launch over the uneven-k stream (P(k) ~ 1/k, k <= 256).
+"""
+from __future__ import annotations
+
+import argparse
+import sys
+import time
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--case", required=True,
+                    choices=["k64", "plain64", "k128", "k256", "gram", "uneven"])
+    ap.add_argument("--nsets", type=int, default=0)
+    ap.add_argument("--launches", type=int, default=2)
+    a = ap.parse_args(argv)
+    import torch
+
+    from . import api
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device=dev).manual_seed(0)
+    t0 = time.perf_counter()
+    if a.case == "gram":
+        m, n, k = 2048, 16384, 128
+        nsets = a.nsets or 8192
+        Phi = torch.randn(m, n, generator=g, device=dev, dtype=torch.float32) / m ** 0.5
+        gf = api.GramFrame(Phi)
+        idx = api.gen_sets(1, 0, nsets, n, k)
+        for _ in range(1 + a.launches):
+            gf.blocks(idx, k)
+    else:
+        m, n = 1024, 4096
+        Phi = torch.randn(m, n, generator=g, device=dev, dtype=torch.float64) / m ** 0.5
+        A = (Phi.T @ Phi).to(torch.float32).contiguous()
+        del Phi
+        if a.case == "uneven":
+            nsets = a.nsets or 100_000
+            off_h, idx_h = api.gen_stream_host(1, 0, nsets, n, kdist=1)
+            idx = torch.from_numpy(idx_h).to(dev)
+            off = torch.from_numpy(off_h).to(dev)
+            out = api.solve(A, idx, offsets=off)
+            for _ in range(a.launches):
+                api.solve(A, idx, offsets=off, out=out)
+        else:
+            k = {"k64": 64, "plain64": 64, "k128": 128, "k256": 256}[a.case]
+            nsets = a.nsets or {64: 200_000, 128: 40_000, 256: 4_000}[k]
+            form = "plain" if a.case == "plain64" else "batched"
+            idx = api.gen_sets(1, 0, nsets, n, k)
+            out = api.solve(A, idx, k=k, form=form)
+            for _ in range(a.launches):
+                api.solve(A, idx, k=k, form=form, out=out)
+    torch.cuda.synchronize()
+    print(f"case {a.case}: {nsets} sets, {1 + a.launches} launches, {time.perf_counter() - t0:.2f} s")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
