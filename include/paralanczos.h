@@ -186,6 +186,19 @@ int pl_calculate_subeigs2(double *mat, int n, int matsize, double *Eigenvalues, 
                           int *subIndex, int subn);
 int pl_calculate_eigs(double *mat, int n, double *Eigenvalues, double *Det);
 
+/* ---- the reference's kernels, launched with the caller's geometry --------
+ * Launches the kernel `name` ("POS_SYM_SUBMATRIX_KER2", "POS_SYM_SUBMATRIX_KER",
+ * "POS_SYM_MAT_KER", "UPPER_KER", "DSG_B", "DSG_B1" or "SG_B1": the
+ * reference's ParaLanczos.h:24-36, same parameter lists) on a grid of grid_x
+ * blocks of block_x x block_y threads with no dynamic shared memory -- what
+ * MATLAB's CUDAKernel does with the reference's PTX (gpu_multi_subsvd2.m:
+ * grid L/128, block 32; gpu_multi_subsvd.m: grid L/minor, block minor/4).
+ * args: pointers to the argument values, cudaLaunchKernel's convention.
+ * Device pointers; asynchronous on `stream`.  The same kernels are in
+ * paralanczos_b200/ParaLanczos.ptx for MATLAB.                               */
+int pl_launch_reference_kernel(const char *name, unsigned grid_x, unsigned block_x, unsigned block_y,
+                               void **args, void *stream);
+
 /* ---- tuning and measurement --------------------------------------------- */
 /* Select variant `variant` of the kernel shape for bin `bin` (see
  * pl_tune_describe); -1 restores the default.                                */

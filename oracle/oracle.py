@@ -76,6 +76,8 @@ def lib():
         L.orc_gershgorin.argtypes = [_dp, _dp, C.c_int, _dp, _dp]
         L.orc_gershgorin.restype = None
         L.orc_bisect_all.argtypes = [_dp, _dp, C.c_int, _dp]
+        L.orc_upper_power.restype = C.c_double
+        L.orc_upper_power.argtypes = [_dp, C.c_int]
         L.orc_dsg_b.restype = None
         L.orc_dsg_b.argtypes = [_dp, _dp, C.c_int, C.c_int, _ip, C.c_int, C.c_int]
         L.orc_bisect_all.restype = None
@@ -242,6 +244,12 @@ def dsg_b(frame, subset, off: int = 0):
     out = np.zeros((n, n))
     lib().orc_dsg_b(_d(out), _d(frame), M, N, _i(subset), n, off)
     return out
+
+
+def upper_power(A) -> float:
+    """UPPER_KER's ||A||_2 estimate (ParaLanczos.cu:1484-1626), all-ones start."""
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    return lib().orc_upper_power(_d(A), A.shape[0])
 
 
 # ----------------------------------------------------------------------------- LAPACK truth

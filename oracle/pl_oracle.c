@@ -29,6 +29,9 @@
  *                          (subgrams[j + i*n] = sum_k Frame[S_i + k*N + off] *
  *                          Frame[S_j + k*N + off], FP64, k ascending), the spec
  *                          of the on-the-fly Gram form.
+ *   - orc_upper_power    : UPPER_KER's norm estimate, ParaLanczos.cu:1484-1626
+ *                          (10 power iterations, Upper = ||A v_9||), with the
+ *                          all-ones start instead of the clock-seeded normal one.
  *   - orc_sturm_count /
  *     orc_bisect_*       : the FP64 Sturm-count bisection the GPU path uses in
  *                          place of TQLRAT (the reference's only Sturm code,
@@ -413,4 +416,28 @@ void orc_dsg_b(double *subgram, const double *frame, int M, int N, const int *su
             subgram[j + i * n] = val;
         }
     }
+}
+
+/* ------------------------------------------------------------------------- */
+/* UPPER_KER restated (ParaLanczos.cu:1484-1626): v = ones/sqrt(n); 10 times  */
+/* w = A v, b = ||w||, v = w / b; returns the last b.  FP64, row-major A.     */
+double orc_upper_power(const double *A, int n)
+{
+    double *v = (double *)malloc(sizeof(double) * n), *w = (double *)malloc(sizeof(double) * n);
+    double b = 0.0;
+    for (int i = 0; i < n; ++i) v[i] = 1.0 / sqrt((double)n);
+    for (int it = 0; it < 10; ++it) {
+        double s = 0.0;
+        for (int i = 0; i < n; ++i) {
+            double acc = 0.0;
+            for (int j = 0; j < n; ++j) acc += A[(long long)i * n + j] * v[j];
+            w[i] = acc;
+            s += acc * acc;
+        }
+        b = sqrt(s);
+        for (int i = 0; i < n; ++i) v[i] = w[i] / b;
+    }
+    free(v);
+    free(w);
+    return b;
 }

@@ -53,6 +53,7 @@ SIGNATURES = {
     "pl_serve_stats": (_i, [_vp, C.POINTER(_d), _i]),
     "pl_serve_reset_stats": (_i, [_vp]),
     "pl_serve_destroy": (_i, [_vp]),
+    "pl_launch_reference_kernel": (_i, [C.c_char_p, C.c_uint, C.c_uint, C.c_uint, C.POINTER(_vp), _vp]),
 }
 
 _lib = None

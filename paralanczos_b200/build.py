@@ -20,6 +20,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libparalanczos_b200.so")
+# PTX of the reference-named kernels, for MATLAB's parallel.gpu.CUDAKernel
+PTX = os.path.join(PKG, "ParaLanczos.ptx")
 UNITS = ["pl_api.cu", "pl_dropin.cu", "pl_compat.cu", "pl_gram.cu", "pl_serve.cu"]
 
 NVCC_FLAGS = [
@@ -87,6 +89,14 @@ def build(verbose_ptxas: bool = False, jobs: int = 0, force: bool = False) -> st
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("link failed")
     os.replace(LIB + ".tmp", LIB)
+    compat = os.path.join(CSRC, "pl_compat.cu")
+    if os.path.exists(compat):
+        r = subprocess.run([cc, "-arch=compute_100a", "-std=c++17", "--expt-relaxed-constexpr",
+                            "-diag-suppress", "177,550", "-ptx", compat, "-o", PTX],
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("ptx failed")
     return LIB
 
 

@@ -16,7 +16,7 @@
 //     the device and solved by the persistent per-bin kernels of the batched
 //     form on the wave's own streams.  A wave is sized to about
 //     PL_SERVE_WAVE_MS (default 20) ms of estimated GPU work: the oldest
-//     unfinished request gets up to half of it, then requests with the
+//     unfinished request gets up to three quarters of it, then requests with the
 //     least remaining work fill the rest, so a large request is split over
 //     waves while small requests that arrive behind it go out in the next
 //     wave instead of waiting for it to finish;
@@ -249,7 +249,7 @@ int wave_scratch(Wave& w, long long nsets) {
 }
 
 // Pieces of the next wave (server lock held): the oldest unfinished request
-// first gets up to half of the wave (no request waits forever), then
+// first gets up to three quarters of the wave (no request waits forever), then
 // requests in order of least remaining work fill the rest, so a small
 // request arriving behind a large one finishes in the next wave while the
 // large one advances a wave at a time.  Every piece has at least one set.
@@ -281,7 +281,7 @@ void form_wave(Server& S, Wave& w) {
       break;
     }
   if (!oldest) return;
-  take(oldest, 0.5 * S.wave_us);
+  take(oldest, 0.75 * S.wave_us);
   std::vector<Request*> order;
   for (Request* r : S.active)
     if (r->next < r->nsets) order.push_back(r);

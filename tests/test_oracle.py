@@ -175,3 +175,19 @@ def test_dsg_b_matches_blas_and_offset():
     assert np.array_equal(G, G.T)
     G1 = O.dsg_b(F, S[:3], off=1)
     assert np.allclose(G1, F[:, S[:3] + 1].T @ F[:, S[:3] + 1], rtol=0, atol=1e-12)
+
+
+def test_upper_power_is_ten_power_iterations():
+    """UPPER_KER restatement (ParaLanczos.cu:1484-1626) with the all-ones start:
+    10 iterations of w = A v, b = ||w||, v = w / b; a lower estimate of ||A||_2
+    that approaches it from below."""
+    rng = np.random.default_rng(1)
+    P = rng.standard_normal((80, 40))
+    A = P.T @ P / 80
+    v = np.ones(40) / np.sqrt(40)
+    for _ in range(10):
+        w = A @ v
+        b = np.linalg.norm(w)
+        v = w / b
+    assert abs(O.upper_power(A) - b) <= 1e-12 * b
+    assert O.upper_power(A) <= np.linalg.eigvalsh(A)[-1] * (1 + 1e-12)
