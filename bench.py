@@ -5,8 +5,9 @@
                     [--workload c2|c3|c4|c5]
 
 The default workload (c2) is the headline configuration described below;
-c3 (uneven k in one launch), c4 (on-the-fly Gram) and c5 (serving) print
-their own JSON line with the same keys (see bench_extra.py).
+c1 (small, through the reference's C entry point), c3 (uneven k in one
+launch), c4 (on-the-fly Gram) and c5 (serving) print their own JSON line with
+the same keys (see bench_extra.py).
 
 Workload (the configuration the headline metric is quoted on): Phi 1024x4096
 with i.i.d. N(0, 1/1024) entries (seeded, generated on the GPU in FP64),
@@ -169,6 +170,23 @@ def cpu_oracle_rate(A_np, idx_np, k, budget_s: float, nthreads: int = 0):
     return n / dt, n, cores, dt, kind
 
 
+def lapack_rate(A64, idx, k, budget_s):
+    """Sets/s of LAPACK dsyevr (extremes only, FP64) on the host, one set at a
+    time, over a bounded sample; BLAS threads as the process has them."""
+    from scipy.linalg import lapack
+    n = len(idx) // k
+    t0 = time.perf_counter()
+    done = 0
+    for s in range(n):
+        S = idx[s * k:(s + 1) * k]
+        w = lapack.dsyevr(A64[np.ix_(S, S)], compute_v=0, range="I", il=1, iu=1)[0]
+        w = lapack.dsyevr(A64[np.ix_(S, S)], compute_v=0, range="I", il=k, iu=k)[0]
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    return done / (time.perf_counter() - t0), done
+
+
 # ----------------------------------------------------------------------------- arms
 
 
@@ -324,10 +342,12 @@ def run_ours(args):
     if rank == 0 and ws == 1 and not args.no_cpu:
         idx_cpu = idx[:200_000 * K].cpu().numpy()
         rate, n, cores, dt, kind = cpu_oracle_rate(A_np, idx_cpu, K, args.cpu_budget)
+        lr, ln = lapack_rate(A_np.astype(np.float64), idx_cpu, K, 5.0)
         cpu = {"value": rate, "unit": "solves/s", "cores": cores, "kind": kind,
                "sample": f"{n} sets of the workload ({dt:.1f} s), OpenMP over {cores} host threads; "
                          "FP64 KER2 recurrence restated + TQLRAT/DET_TRIDIAG"
-                         + (" compiled from the reference source" if kind == "reference" else "")}
+                         + (" compiled from the reference source" if kind == "reference" else ""),
+               "lapack_dsyevr": {"value": lr, "sets": ln, "note": "extremes only, one set per call, FP64"}}
 
     if rank == 0:
         line = {
@@ -374,7 +394,7 @@ def main() -> int:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of CPU-baseline work")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
     ap.add_argument("--rates", default="", help="c5: comma-separated request rates (1/s) to sweep")
     ap.add_argument("--requests", type=int, default=0, help="c5: requests per rate")
     args = ap.parse_args()

@@ -1,8 +1,14 @@
-"""Workloads c3 (uneven k), c4 (on-the-fly Gram) and c5 (serving) of bench.py.
+"""Workloads c1 (small, drop-in path), c3 (uneven k), c4 (on-the-fly Gram) and
+c5 (serving) of bench.py.
 
 Each prints one JSON line with the keys of the headline line (metric, value,
 unit, ms_per_step, e2e, roofline, cpu_baseline, clocks, gpu_launches, ...).
 
+  c1  Phi 128x512 N(0,1/128) (seed 0), A = Phi^T Phi (512 x 512); 10,000 sets
+      of k=16 (generator seed 1) through the reference's C entry point
+      calculate_subeigs3 (host FP64 matrix in, all 16 eigenvalues and the
+      determinant out), beside the batched and plain forms on device buffers;
+      error vs dsyev, CPU oracle and LAPACK dsyevr timed beside it.
   c3  Phi 1024x4096 N(0,1/1024) (seed 0), A = Phi^T Phi FP32; 300,000 sets with
       k in {8,16,24,32,48,64,96,128,192,256}, P(k) ~ 1/k (the library's host
       generator, seed 1); one binned launch per step (device counting sort by k,
@@ -60,6 +66,86 @@ def _timed_steps(fn, steps, warmup, flush, stream):
         torch.cuda.synchronize()
     ms = [a.elapsed_time(b) for a, b in evs]
     return sum(ms) / len(ms), sampler.summary()
+
+
+# ----------------------------------------------------------------------------- c1
+
+
+def run_c1(args):
+    import torch
+
+    from oracle import oracle as O
+    from paralanczos_b200 import api
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    m, n, k, nsets = 128, 512, 16, 10_000
+    rng = np.random.default_rng(B.SEED_PHI)
+    Phi = rng.standard_normal((m, n)) / np.sqrt(m)
+    A64 = Phi.T @ Phi
+    A32 = A64.astype(np.float32)
+    _, idx_h = O.gen_stream(B.SEED_SETS, 0, nsets, n, 0, k, k)
+    idx_h = np.ascontiguousarray(idx_h, dtype=np.int32)
+    eig = np.zeros(nsets * k)
+    det = np.zeros(nsets)
+    api.calculate_subeigs3(A64, nsets * k, n, eig, det, idx_h, k)
+    t = []
+    for _ in range(max(args.steps, 3)):
+        t0 = time.perf_counter()
+        rc = api.calculate_subeigs3(A64, nsets * k, n, eig, det, idx_h, k)
+        t.append(time.perf_counter() - t0)
+        assert rc == 0
+    dropin_s = sum(t) / len(t)
+    # device forms on the same sets
+    A = torch.from_numpy(A32).to(dev)
+    idx = torch.from_numpy(idx_h).to(dev)
+    flush = torch.empty(256 << 18, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    out = api.solve(A, idx, k=k)
+    ms, clocks = _timed_steps(lambda: api.solve(A, idx, k=k, out=out), args.steps, args.warmup, flush, stream)
+    outp = api.solve(A, idx, k=k, form="plain")
+    ms_plain, _ = _timed_steps(lambda: api.solve(A, idx, k=k, form="plain", out=outp), 3, 2, flush, stream)
+    lmin = out["lmin"].cpu().numpy()
+    lmax = out["lmax"].cpu().numpy()
+    worst = worst_all = 0.0
+    for s in range(nsets):
+        S = idx_h[s * k:(s + 1) * k]
+        w = O.dsyev_eigs(A64[np.ix_(S, S)])
+        worst = max(worst, abs(lmin[s] - w[0]) / w[0], abs(lmax[s] - w[-1]) / w[-1])
+        worst_all = max(worst_all, np.max(np.abs(eig[s * k:(s + 1) * k] - w)) / np.max(np.abs(w)))
+    cpu = None
+    if not args.no_cpu:
+        O.use_reference_tqlrat(True)
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        O.batch(A64, idx_h, k=k, nthreads=cores)
+        dt = time.perf_counter() - t0
+        kind = "reference" if O.ref_lib() is not None else "port"
+        lr, ln = B.lapack_rate(A64, idx_h, k, min(5.0, args.cpu_budget))
+        cpu = {"value": nsets / dt, "unit": "solves/s", "cores": cores, "kind": kind,
+               "sample": f"all {nsets} sets ({dt:.2f} s), FP64 KER2 recurrence restated + TQLRAT/DET_TRIDIAG, "
+                         f"OpenMP over {cores} threads",
+               "lapack_dsyevr": {"value": lr, "sets": ln, "note": "extremes only, one set per call"}}
+    line = _line(args, nsets / (ms * 1e-3), ms,
+                 "c1: Phi 128x512 N(0,1/128) seed 0, A 512x512; 10,000 sets k=16 (seed 1); batched form on "
+                 "device buffers; the reference's C entry point timed beside it", {
+                     "e2e": {"value": nsets / dropin_s, "unit": "solves/s",
+                             "h2d_bytes_per_step": int(A64.nbytes + idx_h.nbytes),
+                             "d2h_bytes_per_step": int(eig.nbytes + det.nbytes),
+                             "path": "calculate_subeigs3 (reference C entry point: host FP64 matrix in, all "
+                                     "eigenvalues and determinants out)"},
+                     "gpu_launches": args.steps,
+                     "plain": {"value": nsets / (ms_plain * 1e-3), "ms_per_step": ms_plain},
+                     "accuracy": {"sets_checked": nsets, "max_rel_err_vs_dsyev_extremes": worst,
+                                  "max_err_all_eigenvalues_drop_in": worst_all},
+                     "roofline": {"bound": "fp32", "achieved": 4.0 * k ** 3 * nsets / (ms * 1e-3) / 1e12,
+                                  "peak": api.fp32_peak(), "unit": "TFLOP/s", "traffic": None,
+                                  "note": "10,000 sets fill the GPU for ~0.1 ms: launch-bound"},
+                     "clocks": clocks})
+    line["roofline"]["frac"] = line["roofline"]["achieved"] / line["roofline"]["peak"]
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 # ----------------------------------------------------------------------------- c3
@@ -495,6 +581,6 @@ def run_c5(args):
 def run(args):
     if args.impl == "reference":
         print(json.dumps({"impl": "reference", "unavailable": "the CPU reference arm covers the default c2 "
-                          "workload only; c3-c5 report their CPU sample under cpu_baseline"}))
+                          "workload only; c1, c3-c5 report their CPU sample under cpu_baseline"}))
         return 0
-    return {"c3": run_c3, "c4": run_c4, "c5": run_c5}[args.workload](args)
+    return {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5}[args.workload](args)
