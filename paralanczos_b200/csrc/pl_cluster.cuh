@@ -55,6 +55,17 @@ struct __align__(16) ClusterSmem {
   unsigned long long key[CS];    // breakdown argmax exchange
 };
 
+// Barrier over the set's CTAs.  A one-CTA cluster needs only the CTA barrier
+// (same ordering of its shared-memory writes, without the cluster-scope
+// release/acquire).
+template <int CS>
+__device__ __forceinline__ void set_sync(cg::cluster_group& cl) {
+  if constexpr (CS == 1)
+    __syncthreads();
+  else
+    cl.sync();
+}
+
 // Sum over the CTA, then over the cluster (rank order).  Identical everywhere.
 template <int KB, int CS, int NTC>
 __device__ __forceinline__ double cluster_sum(double x, ClusterSmem<KB, CS, NTC>& sm, int slot,
@@ -71,7 +82,7 @@ __device__ __forceinline__ double cluster_sum(double x, ClusterSmem<KB, CS, NTC>
     ClusterSmem<KB, CS, NTC>* peer = cl.map_shared_rank(&sm, (unsigned)threadIdx.x);
     peer->part[slot][rank] = s;
   }
-  cl.sync();
+  set_sync<CS>(cl);
   double s = sm.part[slot][0];
 #pragma unroll
   for (int r = 1; r < CS; ++r) s += sm.part[slot][r];
@@ -106,7 +117,7 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
   const double badsum = cluster_sum<KB, CS, NTC>(__any_sync(0xffffffffu, bad) ? 1.0 : 0.0, sm, 3, cl, rank);
   if (badsum != 0.0) {
     if (rank == 0 && t == 0) write_failed(out, set, 0, 0, SET_BAD_INDEX);
-    cl.sync();
+    set_sync<CS>(cl);
     return;
   }
 
@@ -245,7 +256,7 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
         }
         cl.map_shared_rank(&sm, (unsigned)t)->key[rank] = m;
       }
-      cl.sync();
+      set_sync<CS>(cl);
       unsigned long long best = 0;
 #pragma unroll
       for (int q = 0; q < CS; ++q) best = sm.key[q] > best ? sm.key[q] : best;
@@ -264,7 +275,7 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
           }
         }
       }
-      cl.sync();
+      set_sync<CS>(cl);
       const float z = sm.vb[nxt][r];
       const double zz = cluster_sum<KB, CS, NTC>(lead ? (double)z * (double)z : 0.0, sm, 2, cl, rank);
       if (t == 0 && rank == 0) sm.ab[j + 1].y = 0x1p-600;  // decoupled block (see sturm_count)
@@ -278,7 +289,7 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
     cur = nxt;
     nxt = old_prv;
   }
-  cl.sync();  // every rank done with the step loop before T is read
+  set_sync<CS>(cl);  // every rank done with the step loop before T is read
 
   // ---- extremes on rank 0: warp 0 lambda_min, warp 1 lambda_max, 33-way -----
   if (rank == 0) {
@@ -311,7 +322,7 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
       }
     }
   }
-  cl.sync();  // rank 0's reads of T and part[] precede the next set's writes
+  set_sync<CS>(cl);  // rank 0's reads of T and part[] precede the next set's writes
 }
 
 }  // namespace pl
