@@ -35,7 +35,7 @@
 // Every mbarrier wait is bounded (%globaltimer); a wait that gives up sets a
 // CTA-wide abort flag and a device status word, every role leaves its loop,
 // outstanding copies and MMAs are drained and TMEM is freed before return.
-// No TMA and no cluster multicast is used.
+// Plain cp.async gathers only: no tensor-memory-accelerator copies of any kind.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
