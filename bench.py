@@ -332,6 +332,22 @@ def run_ours(args):
     h2d = A_h.numel() * 4 + idx_h.numel() * 4
     d2h = NSETS * (8 * 3 + 4)
 
+    # the gather alone (pl_gather_blocks) on 200,000 of the sets
+    gsets = 200_000
+    gidx = idx[:gsets * K]
+    gout = api.gather_blocks(A, gidx, K)
+    ge = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(3)]
+    for a, b in ge:
+        flush.fill_(2.0)
+        a.record(stream)
+        api.gather_blocks(A, gidx, K, out=gout)
+        b.record(stream)
+    torch.cuda.synchronize()
+    g_s = sum(a.elapsed_time(b) for a, b in ge) / len(ge) * 1e-3
+    del gout
+    g_read = gsets * (4.0 * K * (K + 1) / 2 + 4.0 * K) / g_s / 1e9
+    g_write = gsets * 4.0 * K * K / g_s / 1e9
+
     peak_fp32 = api.fp32_peak()
     peaks, peak_src = measured_peaks()
     achieved = flops_per_set(K) * NSETS / (my_ms * 1e-3) / 1e12
@@ -374,6 +390,10 @@ def run_ours(args):
                                 "unit": "GB/s", "frac": gather_gbs / peaks.get("hbm_gbs"),
                                 "peak_source": peak_src,
                                 "algorithmic": "4k(k+1)/2 + 4k + 28 bytes per set over the whole kernel"},
+            "gather_only": {"sets": gsets, "ms": g_s * 1e3, "read_gbs": g_read, "write_gbs": g_write,
+                            "frac_hbm": (g_read + g_write) / peaks.get("hbm_gbs"),
+                            "kernel": "k_gather_blocks (pl_gather_blocks): A[S,S] written as k x k blocks",
+                            "algorithmic": "read 4k(k+1)/2 + 4k bytes, write 4k^2 bytes per set"},
             "clocks": sampler.summary(),
             "wall_s_timed": wall,
         }

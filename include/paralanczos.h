@@ -100,6 +100,14 @@ int pl_solve_host(const float *A, int n, long long lda, const int *idx, const lo
                   long long nsets, int k, int form, double *lmin, double *lmax, double *delta,
                   int *err, double *eig, double *det);
 
+/* The gather alone: blocks[s*k*k + i*k + j] = A[idx[s*k+i], idx[s*k+j]] (device
+ * FP32, row-major blocks), err[s] (nullable) = PL_SET_BAD_INDEX for a set with
+ * an index outside [0, n).  Uniform k <= PL_KMAX; asynchronous on `stream`.
+ * Replaces the reference's per-thread gather LOAD_SMS4H / LOAD_SMS4HF
+ * (ParaLanczos.cu:455-490), which feeds its kernels' private strips.        */
+int pl_gather_blocks(const float *A, int n, long long lda, const int *idx, long long nsets, int k,
+                     float *blocks, int *err, void *stream);
+
 /* Device-side uniform-k index sets from the counter-based generator:
  * idx[s*k ..] = set (first + s) of stream `seed`, k distinct values in [0,n). */
 int pl_gen_sets(unsigned long long seed, long long first, long long nsets, int n, int k, int *idx,

@@ -30,6 +30,7 @@ SIGNATURES = {
     "pl_solve_host": (_i, [_vp, _i, _ll, _vp, _vp, _ll, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
     "pl_solve_noalloc": (_i, [_vp, _i, _ll, _vp, _ll, _i, _vp, _vp, _vp, _vp, _vp]),
     "pl_gen_sets": (_i, [C.c_ulonglong, _ll, _ll, _i, _i, _vp, _vp]),
+    "pl_gather_blocks": (_i, [_vp, _i, _ll, _vp, _ll, _i, _vp, _vp, _vp]),
     "pl_gen_stream_host": (_ll, [C.c_ulonglong, _ll, _ll, _i, _i, _i, _i, _vp, _vp]),
     "pl_convert_f64_f32": (_i, [_vp, _vp, _ll, _vp]),
     "pl_calculate_subeigs3": (_i, [_vp, _i, _i, _vp, _vp, _vp, _i]),

@@ -155,6 +155,19 @@ def solve_host(A, idx, k=None, offsets=None, form="batched", want_all=False):
     return out
 
 
+def gather_blocks(A, idx, k: int, stream=None, out=None):
+    """(nsets, k, k) float32 blocks A[S,S] on the device and int32 status bits."""
+    import torch
+    nsets = idx.numel() // int(k)
+    if out is None:
+        out = (torch.empty((nsets, k, k), dtype=torch.float32, device=A.device),
+               torch.empty(nsets, dtype=torch.int32, device=A.device))
+    st = stream if stream is not None else torch.cuda.current_stream(A.device)
+    check(lib().pl_gather_blocks(A.data_ptr(), A.shape[0], A.stride(0), idx.data_ptr(), nsets, int(k),
+                                 out[0].data_ptr(), out[1].data_ptr(), st.cuda_stream), "pl_gather_blocks")
+    return out
+
+
 def gen_sets(seed: int, first: int, nsets: int, n: int, k: int, device="cuda", stream=None):
     """Uniform-k index sets generated on the device (int32 [nsets*k])."""
     import torch

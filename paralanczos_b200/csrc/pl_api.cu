@@ -691,6 +691,18 @@ int pl_solve_host(const float* A, int n, long long lda, const int* idx, const lo
   return PL_OK;
 }
 
+int pl_gather_blocks(const float* A, int n, long long lda, const int* idx, long long nsets, int k,
+                     float* blocks, int* err, void* stream) {
+  if (nsets < 0 || n <= 0 || lda < n || k < 1 || k > PL_KMAX || k > n) return PL_EINVAL;
+  if (nsets == 0) return PL_OK;
+  if (!A || !idx || !blocks) return PL_EINVAL;
+  const long long g = (long long)device_sms() * 8;
+  k_gather_blocks<<<(unsigned)(nsets < g ? nsets : g), 256, 0, (cudaStream_t)stream>>>(A, n, lda, idx, nsets, k,
+                                                                                      blocks, err);
+  PL_CU(cudaGetLastError());
+  return PL_OK;
+}
+
 int pl_gen_sets(unsigned long long seed, long long first, long long nsets, int n, int k, int* idx,
                 void* stream) {
   if (nsets < 0 || k < 1 || k > n || (nsets > 0 && !idx)) return PL_EINVAL;

@@ -280,6 +280,42 @@ __global__ void k_f64_to_f32(const double* __restrict__ in, float* __restrict__ 
     out[i] = (float)in[i];
 }
 
+// The gather on its own: block s of `blocks` (k x k, row-major) = A[S_s, S_s]
+// (LOAD_SMS4H / LOAD_SMS4HF, ParaLanczos.cu:455-490, without the per-thread
+// 4x4 strips).  One set per block at a time: the set's indices go to shared
+// memory, then every thread copies elements with consecutive output
+// addresses, so the writes are coalesced and all reads of a set are in
+// flight together.  err[s] = SET_BAD_INDEX for an index outside [0, n) (its
+// block is left as zeros).
+__global__ void __launch_bounds__(256) k_gather_blocks(const float* __restrict__ A, int n, long long lda,
+                                                      const int* __restrict__ idx, long long nsets, int k,
+                                                      float* __restrict__ blocks, int* __restrict__ err) {
+  __shared__ int sidx[512];
+  __shared__ int bad;
+  const long long kk = (long long)k * k;
+  for (long long s = blockIdx.x; s < nsets; s += gridDim.x) {
+    if (threadIdx.x == 0) bad = 0;
+    __syncthreads();
+    for (int c = threadIdx.x; c < k; c += blockDim.x) {
+      const int v = __ldg(idx + s * k + c);
+      if (v < 0 || v >= n) bad = 1;
+      sidx[c] = v;
+    }
+    __syncthreads();
+    float* __restrict__ out = blocks + s * kk;
+    if (bad) {
+      for (long long e = threadIdx.x; e < kk; e += blockDim.x) out[e] = 0.f;
+    } else {
+      for (long long e = threadIdx.x; e < kk; e += blockDim.x) {
+        const int r = (int)(e / k), c = (int)(e - (long long)r * k);
+        out[e] = __ldg(A + (size_t)sidx[r] * (size_t)lda + sidx[c]);
+      }
+    }
+    if (threadIdx.x == 0 && err) err[s] = bad ? SET_BAD_INDEX : SET_OK;
+    __syncthreads();
+  }
+}
+
 // Uniform-k index sets from the counter-based generator: one thread per set.
 __global__ void k_gen_sets(unsigned long long seed, long long first, long long nsets, int n, int k,
                            int* __restrict__ idx) {
