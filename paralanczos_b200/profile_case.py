@@ -30,10 +30,17 @@ def main(argv=None) -> int:
                     choices=["k64", "plain64", "k128", "k256", "gram", "uneven"])
     ap.add_argument("--nsets", type=int, default=0)
     ap.add_argument("--launches", type=int, default=2)
+    ap.add_argument("--variant", type=int, default=-2,
+                    help="kernel variant of the case's k bin (pl_tune_describe); default: the tuned one")
     a = ap.parse_args(argv)
     import torch
 
     from . import api
+    if a.variant >= -1:
+        kb = {"k64": 64, "plain64": 64, "k128": 128, "k256": 256, "gram": 128, "uneven": 0}[a.case]
+        b = next(i for i in range(api.num_bins()) if api.bin_kmax(i) >= kb) if kb else 0
+        api.tune_set(b, a.variant)
+        print(f"bin {b}: variant {a.variant} ({api.tune_describe(b, max(a.variant, 0))[1]})")
     dev = torch.device("cuda", 0)
     g = torch.Generator(device=dev).manual_seed(0)
     t0 = time.perf_counter()
