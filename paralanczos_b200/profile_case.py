@@ -13,6 +13,7 @@ Cases:
            sets from the counter-based generator (seed 1); the tuned variant.
   plain64  the same sets through the one-set-per-block form.
   k128     batched form, k = 128 on the same matrix.
+  k192     batched form, k = 192 (one-SM engine of the cluster kernel).
   k256     batched form, k = 256 (thread-block-cluster engine).
   gram     on-the-fly Gram blocks, Phi 2048 x 16384 N(0, 1/2048), k = 128.
   uneven   binned launch over the uneven-k stream (P(k) ~ 1/k, k <= 256).
@@ -27,7 +28,7 @@ import time
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", required=True,
-                    choices=["k64", "plain64", "k128", "k256", "gram", "uneven"])
+                    choices=["k64", "plain64", "k128", "k192", "k256", "gram", "uneven"])
     ap.add_argument("--nsets", type=int, default=0)
     ap.add_argument("--launches", type=int, default=2)
     ap.add_argument("--variant", type=int, default=-2,
@@ -37,7 +38,7 @@ def main(argv=None) -> int:
 
     from . import api
     if a.variant >= -1:
-        kb = {"k64": 64, "plain64": 64, "k128": 128, "k256": 256, "gram": 128, "uneven": 0}[a.case]
+        kb = {"k64": 64, "plain64": 64, "k128": 128, "k192": 192, "k256": 256, "gram": 128, "uneven": 0}[a.case]
         b = next(i for i in range(api.num_bins()) if api.bin_kmax(i) >= kb) if kb else 0
         api.tune_set(b, a.variant)
         print(f"bin {b}: variant {a.variant} ({api.tune_describe(b, max(a.variant, 0))[1]})")
@@ -66,8 +67,8 @@ def main(argv=None) -> int:
             for _ in range(a.launches):
                 api.solve(A, idx, offsets=off, out=out)
         else:
-            k = {"k64": 64, "plain64": 64, "k128": 128, "k256": 256}[a.case]
-            nsets = a.nsets or {64: 200_000, 128: 40_000, 256: 4_000}[k]
+            k = {"k64": 64, "plain64": 64, "k128": 128, "k192": 192, "k256": 256}[a.case]
+            nsets = a.nsets or {64: 200_000, 128: 40_000, 192: 8_000, 256: 4_000}[k]
             form = "plain" if a.case == "plain64" else "batched"
             idx = api.gen_sets(1, 0, nsets, n, k)
             out = api.solve(A, idx, k=k, form=form)
