@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(256) k_gram_split(const float* __restrict__ Ph
 __global__ void __launch_bounds__(NTHREADS, 1)
     k_gram(const char* __restrict__ prep, int n, int kc_total, const int* __restrict__ idx,
            long long nsets, int k, float* __restrict__ blocks, int* __restrict__ gerr,
-           int* __restrict__ status) {
+           int* __restrict__ status, int hold) {
   extern __shared__ unsigned char smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // ---------------- MMA issue (one thread) ----------------
     if ((tid & 31) == 0) {
       uint32_t it = 0, j = 0, G = 0;
-      bool ok = true;
+      bool ok = !hold;  // hold: issue nothing, so every other role's wait runs out
       for (long long set = blockIdx.x; set < nsets && ok; set += gridDim.x, ++j) {
         const uint32_t a = j & 1;
         if (j >= 2 && !mbar_wait(d2empty_bar(a), ((j >> 1) - 1) & 1, abort, status)) {
@@ -540,8 +540,13 @@ int launch_gram(const void* prep, int m, int n, const int* idx, long long nsets,
   const int kc_total = (m + KCH - 1) / KCH;
   long long grid = api_device_sms();
   if (nsets < grid) grid = nsets;
+  // PL_GRAM_TEST_HOLD=1 (tests of the timeout path only): the MMA thread
+  // issues nothing, every bounded wait of the other roles gives up after 2 s,
+  // the kernel frees its TMEM and returns, and the call reports PL_ETIMEDOUT.
+  const char* h = getenv("PL_GRAM_TEST_HOLD");
+  const int hold = (h && h[0] == '1') ? 1 : 0;
   k_gram<<<(unsigned)grid, NTHREADS, kSmemBytes, st>>>((const char*)prep, n, kc_total, idx, nsets, k,
-                                                       blocks, gerr, status);
+                                                       blocks, gerr, status, hold);
   GCU(cudaGetLastError());
   return PL_OK;
 }

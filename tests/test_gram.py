@@ -193,3 +193,39 @@ def test_gram_chunking_is_invisible(tmp_path):
                        check=True, env=env, timeout=300)
         res.append(np.load(path))
     assert np.array_equal(res[0], res[1])
+
+
+_HOLD_SCRIPT = r"""
+import numpy as np, torch, sys
+sys.path.insert(0, {root!r})
+from paralanczos_b200._lib import PLError, PL_ETIMEDOUT
+from paralanczos_b200.api import GramFrame
+import os
+rng = np.random.default_rng(2)
+Phi = (rng.standard_normal((256, 1000)) / 16.0).astype(np.float32)
+S = np.stack([rng.choice(1000, 64, replace=False) for _ in range(300)]).astype(np.int32)
+gf = GramFrame(torch.from_numpy(Phi).cuda())
+idx = torch.from_numpy(S.reshape(-1)).cuda()
+os.environ["PL_GRAM_TEST_HOLD"] = "1"
+try:
+    gf.blocks(idx, 64)
+    print("no timeout")
+    sys.exit(1)
+except PLError as e:
+    assert e.status == PL_ETIMEDOUT, e.status
+os.environ["PL_GRAM_TEST_HOLD"] = "0"
+b, err = gf.blocks(idx, 64)            # the context is still usable
+X = torch.from_numpy(Phi[:, S[0]]).double()
+ref = (X.T @ X).numpy()
+assert np.max(np.abs(b[0].cpu().numpy() - ref)) < 1e-5
+print("ok")
+"""
+
+
+def test_gram_bounded_waits_time_out_cleanly():
+    """With the MMA thread held back (a test switch), every bounded wait of the
+    Gram kernel gives up after 2 s: the call returns PL_ETIMEDOUT, TMEM is
+    freed, and the next call in the same process succeeds."""
+    r = subprocess.run([sys.executable, "-c", _HOLD_SCRIPT.format(root=ROOT)], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
