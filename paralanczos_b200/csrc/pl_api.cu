@@ -133,6 +133,38 @@ size_t scratch_sa() {
   return grid * (CTA / NT) * (NT / 2) * KB * sizeof(double2);
 }
 
+template <int KB, int RPT, int CTA, int REGS, bool ALL>
+cudaError_t launch_sar(const MatrixF32& M, const SetSource& src, const SetOutputs& out,
+                       long long nitems, void* scratch, cudaStream_t st, bool prep) {
+  auto kern = k_sa_solve_r<KB, RPT, CTA, REGS, ALL>;
+  constexpr int GPC = CTA / CfgSA<KB, RPT>::NT;
+  const size_t dsm = sizeof(SASmem<KB, RPT>) * GPC;
+  static int occ = [&] {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
+    cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    return occupancy(kern, CTA, dsm);
+  }();
+  if (prep) {
+    cudaFuncAttributes fa;
+    return cudaFuncGetAttributes(&fa, kern);
+  }
+  const long long grid = grid_for(nitems, GPC, occ);
+  kern<<<(unsigned)grid, CTA, dsm, st>>>(M, src, out, (double2*)scratch);
+  return cudaGetLastError();
+}
+
+template <int KB, int RPT, int CTA, int REGS, bool ALL>
+size_t scratch_sar() {
+  if (ALL) return 0;
+  auto kern = k_sa_solve_r<KB, RPT, CTA, REGS, ALL>;
+  constexpr int NT = CfgSA<KB, RPT>::NT;
+  const size_t dsm = sizeof(SASmem<KB, RPT>) * (CTA / NT);
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
+  cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  const size_t grid = (size_t)device_sms() * occupancy(kern, CTA, dsm);
+  return grid * (CTA / NT) * (NT / 2) * KB * sizeof(double2);
+}
+
 template <int KB, bool ALL>
 cudaError_t launch_plain(const MatrixF32& M, const SetSource& src, const SetOutputs& out,
                          long long nitems, void*, cudaStream_t st, bool prep) {
@@ -225,6 +257,12 @@ struct Variant {
         {launch_sa<KB, RPT, CTA, MINB, false>, launch_sa<KB, RPT, CTA, MINB, true>},          \
         {scratch_sa<KB, RPT, CTA, MINB, false>, scratch_none}                                  \
   }
+#define SAR(KB, RPT, CTA, REGS)                                                              \
+  Variant {                                                                                    \
+    "sharedA KB=" #KB " RPT=" #RPT " CTA=" #CTA " REGS=" #REGS,                                \
+        {launch_sar<KB, RPT, CTA, REGS, false>, launch_sar<KB, RPT, CTA, REGS, true>},        \
+        {scratch_sar<KB, RPT, CTA, REGS, false>, scratch_none}                                 \
+  }
 #define CLUSTER(KB, CS, NTC)                                                                  \
   Variant {                                                                                     \
     "cluster KB=" #KB " CS=" #CS " NTC=" #NTC,                                                  \
@@ -244,7 +282,8 @@ const std::vector<Variant>& variants(int b) {
       {REG(8, 2, 1, 128, 4), REG(8, 1, 1, 128, 4), SA(8, 2, 128, 4)},
       {REG(16, 2, 1, 128, 4), REG(16, 1, 1, 128, 4), SA(16, 2, 128, 4)},
       {REG(32, 2, 1, 128, 3), REG(32, 1, 1, 128, 4), SA(32, 2, 128, 4)},
-      {REG(64, 1, 1, 128, 3), SA(64, 2, 128, 3), REG(64, 1, 1, 128, 2), SA(64, 2, 128, 2)},
+      {REG(64, 1, 1, 128, 3), SA(64, 2, 128, 3), REG(64, 1, 1, 128, 2), SA(64, 2, 128, 2),
+       SAR(64, 2, 96, 224), SAR(64, 2, 128, 224), SAR(64, 2, 64, 200)},
       {SA(128, 1, 128, 3), REG(128, 1, 2, 256, 1), SA(128, 1, 128, 2)},
       {CLUSTER(192, 2, 384), LARGE(256), CLUSTER(192, 4, 192), CLUSTER(192, 1, 384), CLUSTER(192, 1, 768)},
       {CLUSTER(256, 2, 512), LARGE(256), CLUSTER(256, 4, 256), CLUSTER(256, 8, 256)},

@@ -69,9 +69,9 @@ __global__ void __launch_bounds__(CTA, MINB)
 // Batched form, shared-A engine (pl_engine_sa.cuh): persistent, A_S in
 // dynamic shared memory, P in registers.
 // ---------------------------------------------------------------------------
-template <int KB, int RPT, int CTA, int MINB, bool ALL>
-__global__ void __launch_bounds__(CTA, MINB)
-    k_sa_solve(MatrixF32 M, SetSource src, SetOutputs out, double2* __restrict__ qbuf) {
+template <int KB, int RPT, int CTA, bool ALL>
+__device__ __forceinline__ void sa_solve_body(const MatrixF32& M, const SetSource& src, const SetOutputs& out,
+                                              double2* __restrict__ qbuf) {
   using C = CfgSA<KB, RPT>;
   constexpr int GPC = CTA / C::NT;
   constexpr int Q = C::NT / 2;
@@ -119,6 +119,20 @@ __global__ void __launch_bounds__(CTA, MINB)
   if constexpr (!ALL) {
     if (nq > 0) queue_bisect(T, Q, nq, qmeta[gic], g.t, out, g.mask);
   }
+}
+
+template <int KB, int RPT, int CTA, int MINB, bool ALL>
+__global__ void __launch_bounds__(CTA, MINB)
+    k_sa_solve(MatrixF32 M, SetSource src, SetOutputs out, double2* __restrict__ qbuf) {
+  sa_solve_body<KB, RPT, CTA, ALL>(M, src, out, qbuf);
+}
+
+// The same with an explicit register cap per thread (REGS), for CTA shapes
+// whose minimum-blocks bound would round the cap further down.
+template <int KB, int RPT, int CTA, int REGS, bool ALL>
+__global__ void __maxnreg__(REGS) k_sa_solve_r(MatrixF32 M, SetSource src, SetOutputs out,
+                                               double2* __restrict__ qbuf) {
+  sa_solve_body<KB, RPT, CTA, ALL>(M, src, out, qbuf);
 }
 
 // ---------------------------------------------------------------------------
