@@ -333,3 +333,38 @@ def test_rip_sweep_on_gpu_matches_oracle():
     i = int(np.argmax(ref["delta"]))
     assert r.set_id == i and r.n_solved == 3000
     assert abs(r.delta - ref["delta"][i]) <= RTOL * abs(ref["delta"][i])
+
+
+def _correlated_gram(M, N, seed):
+    """Phi = G (I + 0.3 T), T with ones on the first off-diagonals: the serving
+    workload's correlated-column matrix."""
+    rng = np.random.default_rng(seed)
+    G = rng.standard_normal((M, N)) / np.sqrt(M)
+    Phi = G.copy()
+    Phi[:, 1:] += 0.3 * G[:, :-1]
+    Phi[:, :-1] += 0.3 * G[:, 1:]
+    return (Phi.T @ Phi).astype(np.float32)
+
+
+@pytest.mark.parametrize("k", [384, 512])
+def test_large_k_small_lambda_min(k):
+    """k up to 512 from a 1024-row frame: lambda_min ~ (1 - sqrt(k/1024))^2
+    (0.086 at k = 512, condition ~34), the case where FP32 Lanczos error is
+    largest relative to lambda_min; still within 1e-5 of dsyev."""
+    A = cached_gram(1024, 4096, seed=5)
+    o, idx = O.gen_stream(11, 0, 6, A.shape[0], 0, k, k)
+    res = run(A, idx, k=k)
+    assert ok(res["err"])
+    truth = check_vs_dsyev(A, idx, k, res, all_k=False)
+    assert min(t[0] for t in truth) < 0.2
+
+
+@pytest.mark.parametrize("k", [16, 64, 128, 256])
+def test_correlated_and_rademacher_frames(k):
+    """The serving workload's correlated matrix and the Rademacher frame of the
+    Gram workload, through the batched kernels."""
+    for A in (_correlated_gram(1024, 3000, 6), gram(1024, 3000, 7, kind="rad")):
+        o, idx = O.gen_stream(12, 0, 24 if k <= 128 else 6, A.shape[0], 0, k, k)
+        res = run(A, idx, k=k)
+        assert ok(res["err"])
+        check_vs_dsyev(A, idx, k, res, all_k=False)
