@@ -287,7 +287,7 @@ const std::vector<Variant>& variants(int b) {
       {SA(128, 1, 128, 3), REG(128, 1, 2, 256, 1), SA(128, 1, 128, 2)},
       {CLUSTER(192, 2, 384), LARGE(256), CLUSTER(192, 4, 192), CLUSTER(192, 1, 384), CLUSTER(192, 1, 768)},
       {CLUSTER(256, 2, 512), LARGE(256), CLUSTER(256, 4, 256), CLUSTER(256, 8, 256), CLUSTER(256, 2, 256)},
-      {CLUSTER(384, 4, 384), LARGE(512), CLUSTER(384, 8, 192)},
+      {CLUSTER(384, 4, 384), LARGE(512), CLUSTER(384, 8, 192), CLUSTER(384, 6, 256)},
       {CLUSTER(512, 8, 256), LARGE(512), CLUSTER(512, 8, 512)},
   };
   return v[b];
