@@ -369,7 +369,8 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 (FP64 alpha/beta and bisection)", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "precision": "FP32 vectors and matvecs; FP64 alpha/beta accumulation and Sturm bisection",
             "config": {"workload": WORKLOAD, "k": K, "sets_per_gpu": NSETS, "n": N_COLS,
                        "l2": "256 MB index array per step exceeds L2; 256 MB L2 flush between steps",
                        "parallelism": f"replicas x{ws}, set-range sharded" if ws > 1 else "single GPU"},

@@ -44,7 +44,8 @@ KV_C3 = (8, 16, 24, 32, 48, 64, 96, 128, 192, 256)
 def _line(args, metric_value, ms, workload, extra):
     line = {"metric": B.METRIC, "value": metric_value, "unit": "solves/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 alpha/beta and bisection)",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "precision": "FP32 vectors and matvecs; FP64 alpha/beta accumulation and Sturm bisection",
             "data": "synthetic", "config": {"workload": workload}}
     line.update(extra)
     return line
