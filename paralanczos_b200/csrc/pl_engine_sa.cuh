@@ -70,6 +70,11 @@ __device__ __forceinline__ int solve_set_sa(const MatrixF32& M, const int* __res
   float4* __restrict__ my = sm.A + t;  // chunk (q, ch) at my[(q * NCH + ch) * NT]
   float2 Pr[RPT][KB / 2];  // column pairs: packed FP32 (FFMA2) halves the FMA issues
   double fro = 0.0;
+  // A pre-formed block (the Gram form) has contiguous rows: with k % 4 == 0 and
+  // a 16-byte aligned block they are read as float4 (a quarter of the loads,
+  // whose latency is HBM's there).
+  const bool vec = SM.local && (k & 3) == 0 && (SM.lda & 3) == 0 &&
+                   ((reinterpret_cast<uintptr_t>(SM.A) & 15) == 0);
 #pragma unroll
   for (int q = 0; q < RPT; ++q) {
     const int r = t + q * NT;
@@ -78,12 +83,22 @@ __device__ __forceinline__ int solve_set_sa(const MatrixF32& M, const int* __res
 #pragma unroll
     for (int ch = 0; ch < NCH; ++ch) {
       float e[4];
+      if (vec) {
+        const float4 a4 = (rv && 4 * ch < k) ? __ldg(reinterpret_cast<const float4*>(arow) + ch)
+                                             : make_float4(0.f, 0.f, 0.f, 0.f);
+        e[0] = a4.x;
+        e[1] = a4.y;
+        e[2] = a4.z;
+        e[3] = a4.w;
+      } else {
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int c = 4 * ch + u;
-        e[u] = (rv && c < k) ? __ldg(arow + sm.idx[c]) : 0.f;
-        fro += (double)e[u] * (double)e[u];
+        for (int u = 0; u < 4; ++u) {
+          const int c = 4 * ch + u;
+          e[u] = (rv && c < k) ? __ldg(arow + sm.idx[c]) : 0.f;
+        }
       }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) fro += (double)e[u] * (double)e[u];
       Pr[q][2 * ch] = make_float2((rv && 4 * ch == r) ? 1.f : 0.f, (rv && 4 * ch + 1 == r) ? 1.f : 0.f);
       Pr[q][2 * ch + 1] =
           make_float2((rv && 4 * ch + 2 == r) ? 1.f : 0.f, (rv && 4 * ch + 3 == r) ? 1.f : 0.f);
