@@ -37,6 +37,13 @@ struct __align__(16) SASmem {
   double red[6][CfgSA<KB, RPT>::NW];
 };
 
+// Float offset of A_S element (r, c) in the lane-interleaved layout (row
+// r = t + q * NT, column c = 4 * ch + u at ((q * NCH + ch) * NT + t) * 4 + u).
+template <int NT, int NCH>
+__device__ __forceinline__ int sa_at(int r, int c) {
+  return (((r / NT) * NCH + (c >> 2)) * NT + (r % NT)) * 4 + (c & 3);
+}
+
 template <int KB, int RPT, bool ALL>
 __device__ __forceinline__ int solve_set_sa(const MatrixF32& M, const int* __restrict__ S, int k,
                                              long long set, long long off, const SetOutputs& out,
@@ -75,34 +82,73 @@ __device__ __forceinline__ int solve_set_sa(const MatrixF32& M, const int* __res
   // whose latency is HBM's there).
   const bool vec = SM.local && (k & 3) == 0 && (SM.lda & 3) == 0 &&
                    ((reinterpret_cast<uintptr_t>(SM.A) & 15) == 0);
-#pragma unroll
-  for (int q = 0; q < RPT; ++q) {
-    const int r = t + q * NT;
-    const bool rv = r < k;
-    const float* __restrict__ arow = SM.A + (size_t)sm.idx[r] * (size_t)SM.lda;
-#pragma unroll
-    for (int ch = 0; ch < NCH; ++ch) {
-      float e[4];
-      if (vec) {
-        const float4 a4 = (rv && 4 * ch < k) ? __ldg(reinterpret_cast<const float4*>(arow) + ch)
-                                             : make_float4(0.f, 0.f, 0.f, 0.f);
-        e[0] = a4.x;
-        e[1] = a4.y;
-        e[2] = a4.z;
-        e[3] = a4.w;
-      } else {
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int c = 4 * ch + u;
-          e[u] = (rv && c < k) ? __ldg(arow + sm.idx[c]) : 0.f;
-        }
+  bool gathered = false;
+  if constexpr (RPT == 2) {
+    if (!vec) {
+      // A_S is symmetric: load only its upper triangle, k(k+1)/2 of the k^2
+      // random elements (each a separate L1 request and 32-byte sector, the
+      // gather's cost), and store each off-diagonal element twice.  Thread t
+      // takes rows t and KB-1-t, KB+1 elements in all, so the work is even.
+      float* __restrict__ Af = reinterpret_cast<float*>(sm.A);
+      const int r0 = t, r1 = KB - 1 - t;
+      const float* __restrict__ row0 = SM.A + (size_t)sm.idx[r0] * (size_t)SM.lda;
+      const float* __restrict__ row1 = SM.A + (size_t)sm.idx[r1] * (size_t)SM.lda;
+#pragma unroll 8
+      for (int i = 0; i <= KB; ++i) {
+        const bool first = i < KB - t;
+        const int r = first ? r0 : r1;
+        const int c = first ? t + i : i - 1;  // c >= r
+        const float e = (r < k && c < k) ? __ldg((first ? row0 : row1) + sm.idx[c]) : 0.f;
+        const double e2 = (double)e * (double)e;
+        fro += (c == r) ? e2 : 2.0 * e2;
+        Af[sa_at<NT, NCH>(r, c)] = e;
+        if (c != r) Af[sa_at<NT, NCH>(c, r)] = e;
       }
 #pragma unroll
-      for (int u = 0; u < 4; ++u) fro += (double)e[u] * (double)e[u];
-      Pr[q][2 * ch] = make_float2((rv && 4 * ch == r) ? 1.f : 0.f, (rv && 4 * ch + 1 == r) ? 1.f : 0.f);
-      Pr[q][2 * ch + 1] =
-          make_float2((rv && 4 * ch + 2 == r) ? 1.f : 0.f, (rv && 4 * ch + 3 == r) ? 1.f : 0.f);
-      my[(q * NCH + ch) * NT] = make_float4(e[0], e[1], e[2], e[3]);
+      for (int q = 0; q < RPT; ++q) {
+        const int r = t + q * NT;
+        const bool rv = r < k;
+#pragma unroll
+        for (int ch = 0; ch < NCH; ++ch) {
+          Pr[q][2 * ch] =
+              make_float2((rv && 4 * ch == r) ? 1.f : 0.f, (rv && 4 * ch + 1 == r) ? 1.f : 0.f);
+          Pr[q][2 * ch + 1] =
+              make_float2((rv && 4 * ch + 2 == r) ? 1.f : 0.f, (rv && 4 * ch + 3 == r) ? 1.f : 0.f);
+        }
+      }
+      gathered = true;
+    }
+  }
+  if (!gathered) {
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      const int r = t + q * NT;
+      const bool rv = r < k;
+      const float* __restrict__ arow = SM.A + (size_t)sm.idx[r] * (size_t)SM.lda;
+#pragma unroll
+      for (int ch = 0; ch < NCH; ++ch) {
+        float e[4];
+        if (vec) {
+          const float4 a4 = (rv && 4 * ch < k) ? __ldg(reinterpret_cast<const float4*>(arow) + ch)
+                                               : make_float4(0.f, 0.f, 0.f, 0.f);
+          e[0] = a4.x;
+          e[1] = a4.y;
+          e[2] = a4.z;
+          e[3] = a4.w;
+        } else {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int c = 4 * ch + u;
+            e[u] = (rv && c < k) ? __ldg(arow + sm.idx[c]) : 0.f;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) fro += (double)e[u] * (double)e[u];
+        Pr[q][2 * ch] = make_float2((rv && 4 * ch == r) ? 1.f : 0.f, (rv && 4 * ch + 1 == r) ? 1.f : 0.f);
+        Pr[q][2 * ch + 1] =
+            make_float2((rv && 4 * ch + 2 == r) ? 1.f : 0.f, (rv && 4 * ch + 3 == r) ? 1.f : 0.f);
+        my[(q * NCH + ch) * NT] = make_float4(e[0], e[1], e[2], e[3]);
+      }
     }
   }
   const double fro2 = group_sum<NT, NW>(fro, g, sm.red[2]);

@@ -45,6 +45,7 @@
 #include "../../include/paralanczos.h"
 #include "pl_common.cuh"
 #include "pl_internal.h"
+#include "pl_sync.cuh"
 
 namespace pl {
 namespace gram {
@@ -62,7 +63,6 @@ constexpr int NEPI = 128;
 constexpr int NTHREADS = NPROD + NEPI + 32;
 constexpr int SEG = 4;                        // chunks (256 rows of Phi) per D1 segment
 constexpr int TMEM_COLS = 512;                // D1 segment ping-pong + D2 per set, x 2
-constexpr unsigned long long kWaitNs = 2000000000ull;  // bounded waits: 2 s
 
 struct SmemLayout {
   static constexpr int ring = 0;
@@ -92,55 +92,6 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
   d |= (uint64_t)1 << 46;            // descriptor version (sm_100)
   d |= (uint64_t)2 << 61;            // SWIZZLE_128B
   return d;
-}
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ unsigned long long globaltimer() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait for the phase with the given parity.  false: gave up (timeout
-// here, or another role already aborted); the abort flag is then set.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort,
-                                          int* status) {
-  if (mbar_try(bar, parity)) return true;
-  const unsigned long long t0 = globaltimer();
-  for (uint32_t i = 1;; ++i) {
-    if (mbar_try(bar, parity)) return true;
-    if ((i & 31) == 0) {
-      if (*abort) return false;
-      if (globaltimer() - t0 > kWaitNs) {
-        *abort = 1;
-        atomicExch(status, 1);
-        return false;
-      }
-    }
-  }
 }
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
