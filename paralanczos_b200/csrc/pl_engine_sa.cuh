@@ -83,21 +83,27 @@ __device__ __forceinline__ int solve_set_sa(const MatrixF32& M, const int* __res
   const bool vec = SM.local && (k & 3) == 0 && (SM.lda & 3) == 0 &&
                    ((reinterpret_cast<uintptr_t>(SM.A) & 15) == 0);
   bool gathered = false;
-  if constexpr (RPT == 2) {
+  if constexpr (RPT <= 2) {
     if (!vec) {
       // A_S is symmetric: load only its upper triangle, k(k+1)/2 of the k^2
       // random elements (each a separate L1 request and 32-byte sector, the
-      // gather's cost), and store each off-diagonal element twice.  Thread t
-      // takes rows t and KB-1-t, KB+1 elements in all, so the work is even.
+      // gather's cost), and store each off-diagonal element twice.  Rows p and
+      // KB-1-p form a pair with KB+1 upper elements; TPP = 2 / RPT threads
+      // share a pair, so every thread loads about the same number.
+      constexpr int NP = KB / 2, TPP = NT / NP, PER = (KB + TPP) / TPP;
+      static_assert(NP * TPP == NT, "row pairs per group");
       float* __restrict__ Af = reinterpret_cast<float*>(sm.A);
-      const int r0 = t, r1 = KB - 1 - t;
+      const int p = t % NP, i0 = (t / NP) * PER;
+      const int r0 = p, r1 = KB - 1 - p;
       const float* __restrict__ row0 = SM.A + (size_t)sm.idx[r0] * (size_t)SM.lda;
       const float* __restrict__ row1 = SM.A + (size_t)sm.idx[r1] * (size_t)SM.lda;
 #pragma unroll 8
-      for (int i = 0; i <= KB; ++i) {
-        const bool first = i < KB - t;
+      for (int ii = 0; ii < PER; ++ii) {
+        const int i = i0 + ii;
+        if (TPP > 1 && i > KB) break;
+        const bool first = i < KB - p;
         const int r = first ? r0 : r1;
-        const int c = first ? t + i : i - 1;  // c >= r
+        const int c = first ? p + i : i - 1;  // c >= r
         const float e = (r < k && c < k) ? __ldg((first ? row0 : row1) + sm.idx[c]) : 0.f;
         const double e2 = (double)e * (double)e;
         fro += (c == r) ? e2 : 2.0 * e2;
