@@ -125,7 +125,45 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
   float4* __restrict__ my = sm.A + t;  // chunk ch at my[ch * NTC]
   float2 Pr[CPT / 2];
   double fro = 0.0;
-  {
+  if constexpr (CS == 1) {
+    // One CTA holds all of A_S, which is symmetric: load only its upper
+    // triangle (k(k+1)/2 random elements, each its own L1 request) and store
+    // each off-diagonal element twice.  Rows p and KB-1-p form a pair of KB+1
+    // upper elements, shared by TPP threads.
+    constexpr int NP = KB / 2, TPP = NTC / NP, PER = (KB + TPP) / TPP;
+    static_assert(NP * TPP == NTC, "row pairs per CTA");
+    float* __restrict__ Af = reinterpret_cast<float*>(sm.A);
+    // float offset of element (row, col): chunk cc = col / 4 is held by
+    // thread row * TPR + cc % TPR as its chunk cc / TPR
+    auto at = [](int row, int col) {
+      const int cc = col >> 2;
+      return (((cc / TPR) * NTC + row * TPR + cc % TPR) << 2) + (col & 3);
+    };
+    const int p = t % NP, i0 = (t / NP) * PER;
+    const int r0 = p, r1 = KB - 1 - p;
+    const float* __restrict__ row0 = SM.A + (size_t)sm.idx[r0] * (size_t)SM.lda;
+    const float* __restrict__ row1 = SM.A + (size_t)sm.idx[r1] * (size_t)SM.lda;
+#pragma unroll 4
+    for (int ii = 0; ii < PER; ++ii) {
+      const int i = i0 + ii;
+      if (i > KB) break;
+      const bool first = i < KB - p;
+      const int rr = first ? r0 : r1;
+      const int c = first ? p + i : i - 1;  // c >= rr
+      const float e = (rr < k && c < k) ? __ldg((first ? row0 : row1) + sm.idx[c]) : 0.f;
+      const double e2 = (double)e * (double)e;
+      fro += (c == rr) ? e2 : 2.0 * e2;
+      Af[at(rr, c)] = e;
+      if (c != rr) Af[at(c, rr)] = e;
+    }
+    const bool rv = r < k;
+#pragma unroll
+    for (int ch = 0; ch < NCH; ++ch) {
+      const int c = 4 * (g0 + TPR * ch);
+      Pr[2 * ch] = make_float2((rv && c == r) ? 1.f : 0.f, (rv && c + 1 == r) ? 1.f : 0.f);
+      Pr[2 * ch + 1] = make_float2((rv && c + 2 == r) ? 1.f : 0.f, (rv && c + 3 == r) ? 1.f : 0.f);
+    }
+  } else {
     const bool rv = r < k;
     const float* __restrict__ arow = SM.A + (size_t)sm.idx[r] * (size_t)SM.lda;
 #pragma unroll
