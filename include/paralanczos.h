@@ -68,9 +68,10 @@ int pl_last_cuda_error(void);              /* cudaError_t of the last PL_ECUDA *
 /*
  * Solve every set (device pointers).
  *   A       n x n symmetric FP32 matrix, row-major, leading dimension lda >= n
- *           (the batched kernels for k <= 192 read one triangle of each A[S,S]:
- *           for positions r <= c of a set only A[S[r]][S[c]], so an A that is
- *           not exactly symmetric is taken as that triangle mirrored)
+ *           (the batched kernels that keep A[S,S] in shared memory, the tuned
+ *           choice for 32 < k <= 192, read one triangle of it: for positions
+ *           r <= c of a set only A[S[r]][S[c]], so an A that is not exactly
+ *           symmetric is taken as that triangle mirrored)
  *   idx     concatenated 0-based index sets
  *   offsets NULL: uniform k, set s = idx[s*k .. s*k+k-1];
  *           else CSR (nsets+1 entries), set s = idx[offsets[s] .. offsets[s+1])
