@@ -213,7 +213,8 @@ int pl_launch_reference_kernel(const char *name, unsigned grid_x, unsigned block
 
 /* ---- tuning and measurement --------------------------------------------- */
 /* Select variant `variant` of the kernel shape for bin `bin` (see
- * pl_tune_describe); -1 restores the default.                                */
+ * pl_tune_describe); -1 restores the built-in default (the autotuner's
+ * choice on B200).                                                          */
 int pl_tune_set(int bin, int variant);
 /* Writes a description of bin/variant into buf (NUL-terminated); returns the
  * number of variants of `bin`, or 0 for an unknown bin.                      */

@@ -165,6 +165,37 @@ size_t scratch_sar() {
   return grid * (CTA / NT) * (NT / 2) * KB * sizeof(double2);
 }
 
+template <int KB, int CTA, int MINB>
+cudaError_t launch_sa2(const MatrixF32& M, const SetSource& src, const SetOutputs& out,
+                       long long nitems, void* scratch, cudaStream_t st, bool prep) {
+  auto kern = k_sa2_solve<KB, CTA, MINB>;
+  constexpr int GPC = CTA / CfgSA2<KB>::NT;
+  const size_t dsm = sizeof(SA2Smem<KB>) * GPC;
+  static int occ = [&] {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
+    cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    return occupancy(kern, CTA, dsm);
+  }();
+  if (prep) {
+    cudaFuncAttributes fa;
+    return cudaFuncGetAttributes(&fa, kern);
+  }
+  const long long grid = grid_for(nitems, GPC, occ);
+  kern<<<(unsigned)grid, CTA, dsm, st>>>(M, src, out, (double2*)scratch);
+  return cudaGetLastError();
+}
+
+template <int KB, int CTA, int MINB>
+size_t scratch_sa2() {
+  auto kern = k_sa2_solve<KB, CTA, MINB>;
+  constexpr int NT = CfgSA2<KB>::NT;
+  const size_t dsm = sizeof(SA2Smem<KB>) * (CTA / NT);
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
+  cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  const size_t grid = (size_t)device_sms() * occupancy(kern, CTA, dsm);
+  return grid * (CTA / NT) * (NT / 2) * KB * sizeof(double2);
+}
+
 template <int KB, bool ALL>
 cudaError_t launch_plain(const MatrixF32& M, const SetSource& src, const SetOutputs& out,
                          long long nitems, void*, cudaStream_t st, bool prep) {
@@ -263,6 +294,11 @@ struct Variant {
         {launch_sar<KB, RPT, CTA, REGS, false>, launch_sar<KB, RPT, CTA, REGS, true>},        \
         {scratch_sar<KB, RPT, CTA, REGS, false>, scratch_none}                                 \
   }
+#define SA2(KB, CTA, MINB)                                                                   \
+  Variant {                                                                                    \
+    "sharedA 2 threads/row KB=" #KB " CTA=" #CTA " MINB=" #MINB,                               \
+        {launch_sa2<KB, CTA, MINB>, nullptr}, {scratch_sa2<KB, CTA, MINB>, scratch_none}       \
+  }
 #define CLUSTER(KB, CS, NTC)                                                                  \
   Variant {                                                                                     \
     "cluster KB=" #KB " CS=" #CS " NTC=" #NTC,                                                  \
@@ -284,7 +320,7 @@ const std::vector<Variant>& variants(int b) {
       {REG(32, 2, 1, 128, 3), REG(32, 1, 1, 128, 4), SA(32, 2, 128, 4)},
       {REG(64, 1, 1, 128, 3), SA(64, 2, 128, 3), REG(64, 1, 1, 128, 2), SA(64, 2, 128, 2),
        SAR(64, 2, 96, 224), SAR(64, 2, 128, 224), SAR(64, 2, 64, 200)},
-      {SA(128, 1, 128, 3), REG(128, 1, 2, 256, 1), SA(128, 1, 128, 2)},
+      {SA(128, 1, 128, 3), REG(128, 1, 2, 256, 1), SA(128, 1, 128, 2), SA2(128, 128, 2)},
       {CLUSTER(192, 2, 384), LARGE(256), CLUSTER(192, 4, 192), CLUSTER(192, 1, 384), CLUSTER(192, 1, 768)},
       {CLUSTER(256, 2, 512), LARGE(256), CLUSTER(256, 4, 256), CLUSTER(256, 8, 256), CLUSTER(256, 2, 256)},
       {CLUSTER(384, 4, 384), LARGE(512), CLUSTER(384, 8, 192), CLUSTER(384, 6, 256)},
@@ -293,7 +329,10 @@ const std::vector<Variant>& variants(int b) {
   return v[b];
 }
 
-int g_variant[kNumBins] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+// Built-in shape per bin: the autotuner's choices on B200 (tuning.json), so a
+// caller that never runs the Python tuner (a C program, MATLAB) gets them too.
+const int kDefaultVariant[kNumBins] = {0, 0, 1, 5, 3, 3, 4, 3, 0};
+int g_variant[kNumBins] = {0, 0, 1, 5, 3, 3, 4, 3, 0};
 
 int bin_of_k(int k) {
   for (int b = 0; b < kNumBins; ++b)
@@ -779,7 +818,7 @@ int pl_tune_set(int bin, int variant) {
   std::lock_guard<std::mutex> lk(g_mu);
   if (bin < 0 || bin >= kNumBins) return PL_EINVAL;
   if (variant >= (int)variants(bin).size()) return PL_EINVAL;
-  g_variant[bin] = variant < 0 ? 0 : variant;
+  g_variant[bin] = variant < 0 ? kDefaultVariant[bin] : variant;
   return PL_OK;
 }
 

@@ -5,6 +5,7 @@
 #include "pl_cluster.cuh"
 #include "pl_engine.cuh"
 #include "pl_engine_sa.cuh"
+#include "pl_engine_sa2.cuh"
 #include "pl_indexgen.cuh"
 #include "pl_queue.cuh"
 
@@ -133,6 +134,53 @@ template <int KB, int RPT, int CTA, int REGS, bool ALL>
 __global__ void __maxnreg__(REGS) k_sa_solve_r(MatrixF32 M, SetSource src, SetOutputs out,
                                                double2* __restrict__ qbuf) {
   sa_solve_body<KB, RPT, CTA, ALL>(M, src, out, qbuf);
+}
+
+// ---------------------------------------------------------------------------
+// Batched form, shared-A engine with two threads per row (pl_engine_sa2.cuh),
+// extremes only: persistent, A_S in dynamic shared memory, P in registers.
+// ---------------------------------------------------------------------------
+template <int KB, int CTA, int MINB>
+__global__ void __launch_bounds__(CTA, MINB)
+    k_sa2_solve(MatrixF32 M, SetSource src, SetOutputs out, double2* __restrict__ qbuf) {
+  using C = CfgSA2<KB>;
+  constexpr int GPC = CTA / C::NT;
+  constexpr int Q = C::NT / 2;
+  static_assert(CTA % C::NT == 0 && GPC <= 15, "CTA must hold whole groups");
+  extern __shared__ __align__(16) float dsm[];
+  SA2Smem<KB>* smem = reinterpret_cast<SA2Smem<KB>*>(dsm);
+  __shared__ QueueMeta qmeta[GPC][Q];
+  const Grp<C::NT> g = make_group<C::NT>();
+  const int gic = threadIdx.x / C::NT;
+  const long long ng = (long long)gridDim.x * GPC;
+  const long long nitems = item_count(src);
+  const int pbase = src.perm_start ? *src.perm_start : 0;
+  double2* __restrict__ T = qbuf + ((size_t)blockIdx.x * GPC + gic) * (size_t)(Q * KB);
+  int nq = 0;
+  for (long long it = (long long)blockIdx.x * GPC + gic; it < nitems; it += ng) {
+    long long set, off;
+    int k;
+    set_span(src, it, pbase, set, off, k);
+    if (k < 1 || k > KB) {
+      if (g.t == 0) write_failed(out, set, off, 0, SET_BAD_K);
+      continue;
+    }
+    if (g.t == 0) qmeta[gic][nq] = QueueMeta{set, k, 0};
+    const int st = solve_set_sa2<KB>(M, src.idx + off, k, set, off, out, smem[gic], g);
+    if (st >= 0) {
+      const int kq = qmeta[gic][nq].k;
+      for (int i = g.t; i < kq; i += C::NT) T[(size_t)i * Q + nq] = smem[gic].ab[i];
+      if (g.t == 0) qmeta[gic][nq].status = st;
+      ++nq;
+      g.sync();
+      if (nq == Q) {
+        queue_bisect(T, Q, nq, qmeta[gic], g.t, out, g.mask);
+        g.sync();
+        nq = 0;
+      }
+    }
+  }
+  if (nq > 0) queue_bisect(T, Q, nq, qmeta[gic], g.t, out, g.mask);
 }
 
 // ---------------------------------------------------------------------------
