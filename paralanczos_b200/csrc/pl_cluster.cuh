@@ -50,7 +50,8 @@ struct __align__(16) ClusterSmem {
   float wb[KB];                  // w~, formed locally from yb
   int idx[KB];
   double2 ab[KB];                // T (rank 0 reads it for the bisection)
-  double part[4][CS];            // partials from every rank: alpha, ||w||^2, misc, index check
+  double part[4][CS > NTC / 32 ? CS : NTC / 32];  // alpha, ||w||^2, misc, index check: rank
+                                                // partials (warp partials for one CTA)
   double red[NTC / 32];          // warp partials inside the CTA
   unsigned long long key[CS];    // breakdown argmax exchange
 };
@@ -67,26 +68,40 @@ __device__ __forceinline__ void set_sync(cg::cluster_group& cl) {
 }
 
 // Sum over the CTA, then over the cluster (rank order).  Identical everywhere.
+// A one-CTA set skips the CTA-level step: each warp's lane 0 stores its
+// partial in part[slot][warp], one block barrier, and every thread adds the
+// warps' partials in warp order.  (With several CTAs per set, the same scheme
+// -- every warp storing into every peer -- measured slower than one CTA
+// barrier plus one store per peer.)
 template <int KB, int CS, int NTC>
 __device__ __forceinline__ double cluster_sum(double x, ClusterSmem<KB, CS, NTC>& sm, int slot,
                                               cg::cluster_group& cl, int rank) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
   const int w = threadIdx.x >> 5;
-  if ((threadIdx.x & 31) == 0) sm.red[w] = x;
-  __syncthreads();
-  if (threadIdx.x < CS) {
-    double s = sm.red[0];
+  if constexpr (CS == 1) {
+    if ((threadIdx.x & 31) == 0) sm.part[slot][w] = x;
+    __syncthreads();
+    double s = sm.part[slot][0];
 #pragma unroll
-    for (int i = 1; i < NTC / 32; ++i) s += sm.red[i];
-    ClusterSmem<KB, CS, NTC>* peer = cl.map_shared_rank(&sm, (unsigned)threadIdx.x);
-    peer->part[slot][rank] = s;
+    for (int i = 1; i < NTC / 32; ++i) s += sm.part[slot][i];
+    return s;
+  } else {
+    if ((threadIdx.x & 31) == 0) sm.red[w] = x;
+    __syncthreads();
+    if (threadIdx.x < CS) {
+      double s = sm.red[0];
+#pragma unroll
+      for (int i = 1; i < NTC / 32; ++i) s += sm.red[i];
+      ClusterSmem<KB, CS, NTC>* peer = cl.map_shared_rank(&sm, (unsigned)threadIdx.x);
+      peer->part[slot][rank] = s;
+    }
+    set_sync<CS>(cl);
+    double s = sm.part[slot][0];
+#pragma unroll
+    for (int r = 1; r < CS; ++r) s += sm.part[slot][r];
+    return s;
   }
-  set_sync<CS>(cl);
-  double s = sm.part[slot][0];
-#pragma unroll
-  for (int r = 1; r < CS; ++r) s += sm.part[slot][r];
-  return s;
 }
 
 template <int KB, int CS, int NTC>
