@@ -159,9 +159,12 @@ int pl_solve_gram(const void *prep, int m, int n, const int *idx, long long nset
  * arrive: a scheduler thread admits queued requests in arrival order while
  * their indices fit `budget_bytes` of HBM, and runs the admitted work in
  * waves of about PL_SERVE_WAVE_MS (default 20) ms of GPU work -- sets of any
- * matrix and k, binned by k on the device; large requests are split over
- * waves and small ones go first -- with up to `max_waves` waves in flight on
- * their own streams.  Extremes only (lambda_min, lambda_max, delta_k, err).
+ * matrix and k, binned by k on the device; the oldest unfinished request
+ * takes up to PL_SERVE_OLDEST_SHARE (default 0.9) of each wave and the rest
+ * goes to the requests with the least work left, so large requests are split
+ * over waves and small ones go first -- with up to `max_waves` waves in
+ * flight on their own streams.  Extremes only (lambda_min, lambda_max,
+ * delta_k, err).
  * Host buffers; thread-safe.                                                 */
 /* `host_pool_bytes` of pinned memory stage submitted indices and results.    */
 int pl_serve_create(long long budget_bytes, long long host_pool_bytes, int max_waves, void **server);

@@ -16,7 +16,8 @@
 //     the device and solved by the persistent per-bin kernels of the batched
 //     form on the wave's own streams.  A wave is sized to about
 //     PL_SERVE_WAVE_MS (default 20) ms of estimated GPU work: the oldest
-//     unfinished request gets up to three quarters of it, then requests with the
+//     unfinished request gets up to PL_SERVE_OLDEST_SHARE (default 0.9) of
+//     it, then requests with the
 //     least remaining work fill the rest, so a large request is split over
 //     waves while small requests that arrive behind it go out in the next
 //     wave instead of waiting for it to finish;
@@ -201,6 +202,7 @@ struct Server {
   cudaStream_t up = nullptr;   // index uploads at admission
   cudaEvent_t up_ev = nullptr;
   double wave_us = 20000.0;    // GPU work one wave is sized for
+  double oldest_share = 0.9;   // part of a wave the oldest unfinished request may take
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<Request*> pending;  // submitted, not admitted (arrival order)
@@ -249,7 +251,7 @@ int wave_scratch(Wave& w, long long nsets) {
 }
 
 // Pieces of the next wave (server lock held): the oldest unfinished request
-// first gets up to three quarters of the wave (no request waits forever), then
+// first gets up to oldest_share of the wave (no request waits forever), then
 // requests in order of least remaining work fill the rest, so a small
 // request arriving behind a large one finishes in the next wave while the
 // large one advances a wave at a time.  Every piece has at least one set.
@@ -281,7 +283,7 @@ void form_wave(Server& S, Wave& w) {
       break;
     }
   if (!oldest) return;
-  take(oldest, 0.75 * S.wave_us);
+  take(oldest, S.oldest_share * S.wave_us);
   std::vector<Request*> order;
   for (Request* r : S.active)
     if (r->next < r->nsets) order.push_back(r);
@@ -531,6 +533,8 @@ int pl_serve_create(long long budget_bytes, long long host_pool_bytes, int max_w
   S->arena.init((size_t)budget_bytes);
   S->pool.init((size_t)host_pool_bytes);
   if (const char* wm = getenv("PL_SERVE_WAVE_MS")) S->wave_us = std::max(0.1, atof(wm)) * 1000.0;
+  if (const char* os = getenv("PL_SERVE_OLDEST_SHARE"))
+    S->oldest_share = std::min(1.0, std::max(0.05, atof(os)));
   if ((e = cudaStreamCreateWithFlags(&S->up, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaEventCreateWithFlags(&S->up_ev, cudaEventDisableTiming)) != cudaSuccess) {
     destroy(S);
