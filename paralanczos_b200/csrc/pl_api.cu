@@ -331,8 +331,8 @@ const std::vector<Variant>& variants(int b) {
 
 // Built-in shape per bin: the autotuner's choices on B200 (tuning.json), so a
 // caller that never runs the Python tuner (a C program, MATLAB) gets them too.
-const int kDefaultVariant[kNumBins] = {0, 0, 1, 5, 3, 3, 4, 3, 0};
-int g_variant[kNumBins] = {0, 0, 1, 5, 3, 3, 4, 3, 0};
+const int kDefaultVariant[kNumBins] = {0, 0, 2, 5, 3, 3, 4, 3, 0};
+int g_variant[kNumBins] = {0, 0, 2, 5, 3, 3, 4, 3, 0};
 
 int bin_of_k(int k) {
   for (int b = 0; b < kNumBins; ++b)
