@@ -232,10 +232,10 @@ cudaError_t launch_large(const MatrixF32& M, const SetSource& src, const SetOutp
   return cudaGetLastError();
 }
 
-template <int KB, int CS, int NTC>
+template <int KB, int CS, int NTC, int RPT = 1>
 cudaError_t launch_cluster(const MatrixF32& M, const SetSource& src, const SetOutputs& out,
                            long long nitems, void*, cudaStream_t st, bool prep) {
-  auto kern = k_cluster_solve<KB, CS, NTC>;
+  auto kern = k_cluster_solve<KB, CS, NTC, RPT>;
   const size_t dsm = sizeof(ClusterSmem<KB, CS, NTC>);
   static int maxcl = [&] {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
@@ -304,6 +304,12 @@ struct Variant {
     "cluster KB=" #KB " CS=" #CS " NTC=" #NTC,                                                  \
         {launch_cluster<KB, CS, NTC>, nullptr}, {scratch_none, scratch_none}                    \
   }
+// RPT rows per thread (each with KB / TPR columns of P)
+#define CLUSTERR(KB, CS, NTC, RPT)                                                            \
+  Variant {                                                                                     \
+    "cluster KB=" #KB " CS=" #CS " NTC=" #NTC " RPT=" #RPT,                                     \
+        {launch_cluster<KB, CS, NTC, RPT>, nullptr}, {scratch_none, scratch_none}               \
+  }
 #define LARGE(KM) \
   Variant {                                                                             \
     "large KM=" #KM " CTA=256", {launch_large<KM, false>, launch_large<KM, true>},      \
@@ -321,18 +327,20 @@ const std::vector<Variant>& variants(int b) {
       {REG(64, 1, 1, 128, 3), SA(64, 2, 128, 3), REG(64, 1, 1, 128, 2), SA(64, 2, 128, 2),
        SAR(64, 2, 96, 224), SAR(64, 2, 128, 224), SAR(64, 2, 64, 200)},
       {SA(128, 1, 128, 3), REG(128, 1, 2, 256, 1), SA(128, 1, 128, 2), SA2(128, 128, 2)},
-      {CLUSTER(192, 2, 384), LARGE(256), CLUSTER(192, 4, 192), CLUSTER(192, 1, 384), CLUSTER(192, 1, 768)},
-      {CLUSTER(256, 2, 512), LARGE(256), CLUSTER(256, 4, 256), CLUSTER(256, 8, 256), CLUSTER(256, 2, 256)},
-      {CLUSTER(384, 4, 384), LARGE(512), CLUSTER(384, 8, 192), CLUSTER(384, 6, 256)},
-      {CLUSTER(512, 8, 256), LARGE(512), CLUSTER(512, 8, 512)},
+      {CLUSTER(192, 2, 384), LARGE(256), CLUSTER(192, 4, 192), CLUSTER(192, 1, 384), CLUSTER(192, 1, 768),
+       CLUSTERR(192, 1, 384, 2)},
+      {CLUSTER(256, 2, 512), LARGE(256), CLUSTER(256, 4, 256), CLUSTER(256, 8, 256), CLUSTER(256, 2, 256),
+       CLUSTERR(256, 2, 256, 2)},
+      {CLUSTER(384, 4, 384), LARGE(512), CLUSTER(384, 8, 192), CLUSTER(384, 6, 256), CLUSTERR(384, 6, 256, 2)},
+      {CLUSTER(512, 8, 256), LARGE(512), CLUSTER(512, 8, 512), CLUSTERR(512, 8, 256, 2)},
   };
   return v[b];
 }
 
 // Built-in shape per bin: the autotuner's choices on B200 (tuning.json), so a
 // caller that never runs the Python tuner (a C program, MATLAB) gets them too.
-const int kDefaultVariant[kNumBins] = {0, 0, 2, 5, 3, 3, 4, 3, 0};
-int g_variant[kNumBins] = {0, 0, 2, 5, 3, 3, 4, 3, 0};
+const int kDefaultVariant[kNumBins] = {0, 0, 2, 5, 3, 5, 5, 4, 3};
+int g_variant[kNumBins] = {0, 0, 2, 5, 3, 5, 5, 4, 3};
 
 int bin_of_k(int k) {
   for (int b = 0; b < kNumBins; ++b)

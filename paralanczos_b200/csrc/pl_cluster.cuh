@@ -15,12 +15,15 @@
 // w~ = y - alpha v_j - beta_j v_{j-1} locally), one carries the rows of w with
 // the ||w||^2 partials.
 //
-// Thread mapping inside a CTA: NTC threads, TPR = NTC / R threads per row;
+// Thread mapping inside a CTA: NTC threads; a thread holds RPT of the CTA's
+// R rows (rows ls, ls + R/RPT, ...), TPR = NTC * RPT / R threads share a row;
 // thread g = t % TPR of a row owns the float4 column chunks g, g + TPR,
-// g + 2 TPR, ... (CPT = KB / TPR columns), so the TPR threads of a row read
-// adjacent 16-byte chunks of a broadcast vector: conflict-free shared-memory
-// loads.  Row partial sums are combined with xor-shuffles over the TPR lanes
-// (TPR divides 32).
+// g + 2 TPR, ... (CPT = KB / TPR columns of each of its rows), so the TPR
+// threads of a row read adjacent 16-byte chunks of a broadcast vector:
+// conflict-free shared-memory loads.  Row partial sums are combined with
+// xor-shuffles over the TPR lanes (TPR divides 32).  With RPT = 2 a thread
+// holds as much of P as with one row of twice the columns, but reads half of
+// each broadcast vector per step.
 #pragma once
 #include <cooperative_groups.h>
 
@@ -31,14 +34,15 @@ namespace pl {
 
 namespace cg = cooperative_groups;
 
-template <int KB, int CS, int NTC>
+template <int KB, int CS, int NTC, int RPT = 1>
 struct CfgC {
   static constexpr int R = KB / CS;       // rows per CTA
-  static constexpr int TPR = NTC / R;     // threads per row
-  static constexpr int CPT = KB / TPR;    // columns per thread
-  static constexpr int NCH = CPT / 4;     // float4 chunks per thread
+  static constexpr int RS = R / RPT;      // row slots: a thread holds rows ls, ls + RS, ...
+  static constexpr int TPR = NTC / RS;    // threads per row
+  static constexpr int CPT = KB / TPR;    // columns per thread (of each of its rows)
+  static constexpr int NCH = CPT / 4;     // float4 chunks per thread and row
   static constexpr int NWC = NTC / 32;    // warps per CTA
-  static_assert(KB % CS == 0 && NTC % R == 0 && KB % TPR == 0, "bad shape");
+  static_assert(KB % CS == 0 && R % RPT == 0 && NTC % RS == 0 && KB % TPR == 0, "bad shape");
   static_assert(32 % TPR == 0 && CPT % 4 == 0, "bad shape");
 };
 
@@ -104,16 +108,18 @@ __device__ __forceinline__ double cluster_sum(double x, ClusterSmem<KB, CS, NTC>
   }
 }
 
-template <int KB, int CS, int NTC>
+template <int KB, int CS, int NTC, int RPT = 1>
 __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int* __restrict__ S,
                                                   int k, long long set, const SetOutputs& out,
                                                   ClusterSmem<KB, CS, NTC>& sm,
                                                   cg::cluster_group& cl, int rank) {
-  using C = CfgC<KB, CS, NTC>;
-  constexpr int R = C::R, TPR = C::TPR, CPT = C::CPT, NCH = C::NCH;
+  using C = CfgC<KB, CS, NTC, RPT>;
+  constexpr int R = C::R, RS = C::RS, TPR = C::TPR, CPT = C::CPT, NCH = C::NCH;
   const int t = threadIdx.x;
-  const int lr = t / TPR;              // local row
-  const int r = rank * R + lr;         // global row
+  const int ls = t / TPR;              // row slot: local rows ls + q * RS
+  int r[RPT];                          // global rows
+#pragma unroll
+  for (int q = 0; q < RPT; ++q) r[q] = rank * R + ls + q * RS;
   const int g0 = t % TPR;              // owned chunks g0 + TPR * ch
   const bool lead = g0 == 0;
   const unsigned rmask = (TPR == 32) ? 0xffffffffu : (((1u << TPR) - 1u) << ((t & 31) / TPR * TPR));
@@ -137,8 +143,8 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
   }
 
   // ---- gather own rows of A_S into shared memory; P = I ----------------------
-  float4* __restrict__ my = sm.A + t;  // chunk ch at my[ch * NTC]
-  float2 Pr[CPT / 2];
+  float4* __restrict__ my = sm.A + t;  // chunk (q, ch) at my[(q * NCH + ch) * NTC]
+  float2 Pr[RPT][CPT / 2];
   double fro = 0.0;
   if constexpr (CS == 1) {
     // One CTA holds all of A_S, which is symmetric: load only its upper
@@ -148,11 +154,11 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
     constexpr int NP = KB / 2, TPP = NTC / NP, PER = (KB + TPP) / TPP;
     static_assert(NP * TPP == NTC, "row pairs per CTA");
     float* __restrict__ Af = reinterpret_cast<float*>(sm.A);
-    // float offset of element (row, col): chunk cc = col / 4 is held by
-    // thread row * TPR + cc % TPR as its chunk cc / TPR
+    // float offset of element (row, col): chunk cc = col / 4 of row
+    // q * RS + ls is held by thread ls * TPR + cc % TPR as its chunk (q, cc / TPR)
     auto at = [](int row, int col) {
       const int cc = col >> 2;
-      return (((cc / TPR) * NTC + row * TPR + cc % TPR) << 2) + (col & 3);
+      return ((((row / RS) * NCH + cc / TPR) * NTC + (row % RS) * TPR + cc % TPR) << 2) + (col & 3);
     };
     const int p = t % NP, i0 = (t / NP) * PER;
     const int r0 = p, r1 = KB - 1 - p;
@@ -171,29 +177,37 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
       Af[at(rr, c)] = e;
       if (c != rr) Af[at(c, rr)] = e;
     }
-    const bool rv = r < k;
 #pragma unroll
-    for (int ch = 0; ch < NCH; ++ch) {
-      const int c = 4 * (g0 + TPR * ch);
-      Pr[2 * ch] = make_float2((rv && c == r) ? 1.f : 0.f, (rv && c + 1 == r) ? 1.f : 0.f);
-      Pr[2 * ch + 1] = make_float2((rv && c + 2 == r) ? 1.f : 0.f, (rv && c + 3 == r) ? 1.f : 0.f);
+    for (int q = 0; q < RPT; ++q) {
+      const bool rv = r[q] < k;
+#pragma unroll
+      for (int ch = 0; ch < NCH; ++ch) {
+        const int c = 4 * (g0 + TPR * ch);
+        Pr[q][2 * ch] = make_float2((rv && c == r[q]) ? 1.f : 0.f, (rv && c + 1 == r[q]) ? 1.f : 0.f);
+        Pr[q][2 * ch + 1] =
+            make_float2((rv && c + 2 == r[q]) ? 1.f : 0.f, (rv && c + 3 == r[q]) ? 1.f : 0.f);
+      }
     }
   } else {
-    const bool rv = r < k;
-    const float* __restrict__ arow = SM.A + (size_t)sm.idx[r] * (size_t)SM.lda;
 #pragma unroll
-    for (int ch = 0; ch < NCH; ++ch) {
-      float e[4];
+    for (int q = 0; q < RPT; ++q) {
+      const bool rv = r[q] < k;
+      const float* __restrict__ arow = SM.A + (size_t)sm.idx[r[q]] * (size_t)SM.lda;
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int c = 4 * (g0 + TPR * ch) + u;
-        e[u] = (rv && c < k) ? __ldg(arow + sm.idx[c]) : 0.f;
-        fro += (double)e[u] * (double)e[u];
+      for (int ch = 0; ch < NCH; ++ch) {
+        float e[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int c = 4 * (g0 + TPR * ch) + u;
+          e[u] = (rv && c < k) ? __ldg(arow + sm.idx[c]) : 0.f;
+          fro += (double)e[u] * (double)e[u];
+        }
+        my[(q * NCH + ch) * NTC] = make_float4(e[0], e[1], e[2], e[3]);
+        const int c = 4 * (g0 + TPR * ch);
+        Pr[q][2 * ch] = make_float2((rv && c == r[q]) ? 1.f : 0.f, (rv && c + 1 == r[q]) ? 1.f : 0.f);
+        Pr[q][2 * ch + 1] =
+            make_float2((rv && c + 2 == r[q]) ? 1.f : 0.f, (rv && c + 3 == r[q]) ? 1.f : 0.f);
       }
-      my[ch * NTC] = make_float4(e[0], e[1], e[2], e[3]);
-      const int c = 4 * (g0 + TPR * ch);
-      Pr[2 * ch] = make_float2((rv && c == r) ? 1.f : 0.f, (rv && c + 1 == r) ? 1.f : 0.f);
-      Pr[2 * ch + 1] = make_float2((rv && c + 2 == r) ? 1.f : 0.f, (rv && c + 3 == r) ? 1.f : 0.f);
     }
   }
   const double fro2 = cluster_sum<KB, CS, NTC>(fro, sm, 2, cl, rank);
@@ -203,7 +217,9 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
   // (scaled by scp); w is published into vb[nxt].  Peers write vb[nxt] and yb
   // only after a cluster barrier that follows every read of the old contents.
   const float v0 = (float)(1.0 / sqrt((double)k));
-  float v = r < k ? v0 : 0.f;
+  float v[RPT];
+#pragma unroll
+  for (int q = 0; q < RPT; ++q) v[q] = r[q] < k ? v0 : 0.f;
   for (int c = t; c < KB; c += NTC) {
     sm.vb[0][c] = c < k ? v0 : 0.f;
     sm.vb[1][c] = 0.f;
@@ -215,29 +231,47 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
   __syncthreads();
 
   for (int j = 0; j < k; ++j) {
-    // P -= v v^T and y = A v over the owned row slice
-    float2 ya = make_float2(0.f, 0.f), yb = make_float2(0.f, 0.f);
-    const float cq = -v * sc;
-    const float2 nc = make_float2(cq, cq);
+    // P -= v v^T and y = A v over the owned row slices
+    float2 ya[RPT], yb[RPT], nc[RPT];
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      const float cq = -v[q] * sc;
+      nc[q] = make_float2(cq, cq);
+      ya[q] = make_float2(0.f, 0.f);
+      yb[q] = make_float2(0.f, 0.f);
+    }
 #pragma unroll
     for (int ch = 0; ch < NCH; ++ch) {
       const float4 b4 = *reinterpret_cast<const float4*>(&sm.vb[cur][4 * (g0 + TPR * ch)]);
-      const float4 a4 = my[ch * NTC];
       const float2 b01 = make_float2(b4.x, b4.y), b23 = make_float2(b4.z, b4.w);
-      Pr[2 * ch] = __ffma2_rn(nc, b01, Pr[2 * ch]);
-      Pr[2 * ch + 1] = __ffma2_rn(nc, b23, Pr[2 * ch + 1]);
-      ya = __ffma2_rn(make_float2(a4.x, a4.y), b01, ya);
-      yb = __ffma2_rn(make_float2(a4.z, a4.w), b23, yb);
-    }
-    float y = ((ya.x + ya.y) + (yb.x + yb.y)) * sc;
 #pragma unroll
-    for (int o = TPR / 2; o > 0; o >>= 1) y += __shfl_xor_sync(rmask, y, o);
+      for (int q = 0; q < RPT; ++q) {
+        const float4 a4 = my[(q * NCH + ch) * NTC];
+        Pr[q][2 * ch] = __ffma2_rn(nc[q], b01, Pr[q][2 * ch]);
+        Pr[q][2 * ch + 1] = __ffma2_rn(nc[q], b23, Pr[q][2 * ch + 1]);
+        ya[q] = __ffma2_rn(make_float2(a4.x, a4.y), b01, ya[q]);
+        yb[q] = __ffma2_rn(make_float2(a4.z, a4.w), b23, yb[q]);
+      }
+    }
+    float y[RPT];
+    double ap = 0.0;
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      y[q] = ((ya[q].x + ya[q].y) + (yb[q].x + yb[q].y)) * sc;
+#pragma unroll
+      for (int o = TPR / 2; o > 0; o >>= 1) y[q] += __shfl_xor_sync(rmask, y[q], o);
+      ap = q == 0 ? (double)v[0] * (double)y[0] : fma((double)v[q], (double)y[q], ap);
+    }
     // publish the owned rows of y with the alpha partial: one cluster barrier
     if (lead) {
 #pragma unroll
-      for (int q = 0; q < CS; ++q) cl.map_shared_rank(&sm, (unsigned)q)->yb[r] = y;
+      for (int p = 0; p < CS; ++p) {
+        ClusterSmem<KB, CS, NTC>* peer = cl.map_shared_rank(&sm, (unsigned)p);
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) peer->yb[r[q]] = y[q];
+      }
     }
-    const double alpha = cluster_sum<KB, CS, NTC>(lead ? (double)v * (double)y : 0.0, sm, 0, cl, rank);
+    const double alpha = cluster_sum<KB, CS, NTC>(lead ? ap : 0.0, sm, 0, cl, rank);
     const float af = (float)alpha;
 
     // w~ = y - alpha v_j - beta_j v_{j-1}, every element formed locally
@@ -245,22 +279,40 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
       sm.wb[c] = fmaf(-af, sc * sm.vb[cur][c], fmaf(-bprev, scp * sm.vb[prv][c], sm.yb[c]));
     __syncthreads();
 
-    // w = P w~ over the owned row slice
-    float2 wa = make_float2(0.f, 0.f), wc = make_float2(0.f, 0.f);
+    // w = P w~ over the owned row slices
+    float2 wa[RPT], wc[RPT];
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      wa[q] = make_float2(0.f, 0.f);
+      wc[q] = make_float2(0.f, 0.f);
+    }
 #pragma unroll
     for (int ch = 0; ch < NCH; ++ch) {
       const float4 x4 = *reinterpret_cast<const float4*>(&sm.wb[4 * (g0 + TPR * ch)]);
-      wa = __ffma2_rn(Pr[2 * ch], make_float2(x4.x, x4.y), wa);
-      wc = __ffma2_rn(Pr[2 * ch + 1], make_float2(x4.z, x4.w), wc);
-    }
-    float w = (wa.x + wa.y) + (wc.x + wc.y);
 #pragma unroll
-    for (int o = TPR / 2; o > 0; o >>= 1) w += __shfl_xor_sync(rmask, w, o);
+      for (int q = 0; q < RPT; ++q) {
+        wa[q] = __ffma2_rn(Pr[q][2 * ch], make_float2(x4.x, x4.y), wa[q]);
+        wc[q] = __ffma2_rn(Pr[q][2 * ch + 1], make_float2(x4.z, x4.w), wc[q]);
+      }
+    }
+    float w[RPT];
+    double bp = 0.0;
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      w[q] = (wa[q].x + wa[q].y) + (wc[q].x + wc[q].y);
+#pragma unroll
+      for (int o = TPR / 2; o > 0; o >>= 1) w[q] += __shfl_xor_sync(rmask, w[q], o);
+      bp = q == 0 ? (double)w[0] * (double)w[0] : fma((double)w[q], (double)w[q], bp);
+    }
     if (lead) {
 #pragma unroll
-      for (int q = 0; q < CS; ++q) cl.map_shared_rank(&sm, (unsigned)q)->vb[nxt][r] = w;
+      for (int p = 0; p < CS; ++p) {
+        ClusterSmem<KB, CS, NTC>* peer = cl.map_shared_rank(&sm, (unsigned)p);
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) peer->vb[nxt][r[q]] = w[q];
+      }
     }
-    const double b2v = cluster_sum<KB, CS, NTC>(lead ? (double)w * (double)w : 0.0, sm, 1, cl, rank);
+    const double b2v = cluster_sum<KB, CS, NTC>(lead ? bp : 0.0, sm, 1, cl, rank);
     if (t == 0 && rank == 0) {
       sm.ab[j].x = alpha;
       if (j + 1 < k) sm.ab[j + 1].y = b2v;
@@ -275,24 +327,30 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
       scp = sc;
       sc = 1.0f / bf;
       bprev = bf;
-      v = w * sc;
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) v[q] = w[q] * sc;
     } else {
       // Breakdown: restart from the column of P with the largest diagonal
       // (cluster-wide argmax, ties to the smaller row), published into vb[nxt].
       status |= SET_BREAKDOWN;
       unsigned long long kk = 0ull;
-      if (r < k && ((r >> 2) - g0) % TPR == 0) {  // this thread owns column r
-        float d = 0.f;
 #pragma unroll
-        for (int ch = 0; ch < NCH; ++ch) {
-          const int c = 4 * (g0 + TPR * ch);
-          if (c == r) d = Pr[2 * ch].x;
-          if (c + 1 == r) d = Pr[2 * ch].y;
-          if (c + 2 == r) d = Pr[2 * ch + 1].x;
-          if (c + 3 == r) d = Pr[2 * ch + 1].y;
+      for (int q = 0; q < RPT; ++q) {
+        if (r[q] < k && (r[q] >> 2) % TPR == g0) {  // this thread owns column r[q] of row r[q]
+          float d = 0.f;
+#pragma unroll
+          for (int ch = 0; ch < NCH; ++ch) {
+            const int c = 4 * (g0 + TPR * ch);
+            if (c == r[q]) d = Pr[q][2 * ch].x;
+            if (c + 1 == r[q]) d = Pr[q][2 * ch].y;
+            if (c + 2 == r[q]) d = Pr[q][2 * ch + 1].x;
+            if (c + 3 == r[q]) d = Pr[q][2 * ch + 1].y;
+          }
+          d = fmaxf(d, 0.f);
+          const unsigned long long kq =
+              ((unsigned long long)__float_as_uint(d) << 32) | (unsigned)(0x7fffffff - r[q]);
+          kk = kq > kk ? kq : kk;
         }
-        d = fmaxf(d, 0.f);
-        kk = ((unsigned long long)__float_as_uint(d) << 32) | (unsigned)(0x7fffffff - r);
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
@@ -314,28 +372,38 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
 #pragma unroll
       for (int q = 0; q < CS; ++q) best = sm.key[q] > best ? sm.key[q] : best;
       const int mrow = 0x7fffffff - (int)(best & 0xffffffffu);
-      if (mrow / R == rank && lr == mrow % R) {
 #pragma unroll
-        for (int q = 0; q < CS; ++q) {
-          float* dst = cl.map_shared_rank(&sm, (unsigned)q)->vb[nxt];
+      for (int q = 0; q < RPT; ++q) {
+        if (r[q] == mrow) {
 #pragma unroll
-          for (int ch = 0; ch < NCH; ++ch) {
-            const int c = 4 * (g0 + TPR * ch);
-            dst[c] = Pr[2 * ch].x;
-            dst[c + 1] = Pr[2 * ch].y;
-            dst[c + 2] = Pr[2 * ch + 1].x;
-            dst[c + 3] = Pr[2 * ch + 1].y;
+          for (int p = 0; p < CS; ++p) {
+            float* dst = cl.map_shared_rank(&sm, (unsigned)p)->vb[nxt];
+#pragma unroll
+            for (int ch = 0; ch < NCH; ++ch) {
+              const int c = 4 * (g0 + TPR * ch);
+              dst[c] = Pr[q][2 * ch].x;
+              dst[c + 1] = Pr[q][2 * ch].y;
+              dst[c + 2] = Pr[q][2 * ch + 1].x;
+              dst[c + 3] = Pr[q][2 * ch + 1].y;
+            }
           }
         }
       }
       set_sync<CS>(cl);
-      const float z = sm.vb[nxt][r];
-      const double zz = cluster_sum<KB, CS, NTC>(lead ? (double)z * (double)z : 0.0, sm, 2, cl, rank);
+      float z[RPT];
+      double zp = 0.0;
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) {
+        z[q] = sm.vb[nxt][r[q]];
+        zp = q == 0 ? (double)z[0] * (double)z[0] : fma((double)z[q], (double)z[q], zp);
+      }
+      const double zz = cluster_sum<KB, CS, NTC>(lead ? zp : 0.0, sm, 2, cl, rank);
       if (t == 0 && rank == 0) sm.ab[j + 1].y = 0x1p-600;  // decoupled block (see sturm_count)
       scp = sc;
       sc = 1.0f / sqrtf((float)zz);
       bprev = 0.f;
-      v = z * sc;
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) v[q] = z[q] * sc;
     }
     const int old_prv = prv;
     prv = cur;

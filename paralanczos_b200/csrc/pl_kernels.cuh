@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(256, 1)
 // Large-k batched form on thread-block clusters (pl_cluster.cuh): persistent,
 // one set per cluster of CS CTAs at a time.
 // ---------------------------------------------------------------------------
-template <int KB, int CS, int NTC>
+template <int KB, int CS, int NTC, int RPT = 1>
 __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(NTC, 1)
     k_cluster_solve(MatrixF32 M, SetSource src, SetOutputs out) {
   extern __shared__ __align__(16) float dsm[];
@@ -262,7 +262,7 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(NTC, 1)
       if (rank == 0 && threadIdx.x == 0) write_failed(out, set, off, 0, SET_BAD_K);
       continue;
     }
-    cluster_solve_set<KB, CS, NTC>(M, src.idx + off, k, set, out, sm, cl, rank);
+    cluster_solve_set<KB, CS, NTC, RPT>(M, src.idx + off, k, set, out, sm, cl, rank);
   }
 }
 
