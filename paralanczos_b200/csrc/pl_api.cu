@@ -332,7 +332,7 @@ const std::vector<Variant>& variants(int b) {
       {CLUSTER(256, 2, 512), LARGE(256), CLUSTER(256, 4, 256), CLUSTER(256, 8, 256), CLUSTER(256, 2, 256),
        CLUSTERR(256, 2, 256, 2), CLUSTERR(256, 2, 256, 4)},
       {CLUSTER(384, 4, 384), LARGE(512), CLUSTER(384, 8, 192), CLUSTER(384, 6, 256), CLUSTERR(384, 6, 256, 2),
-       CLUSTERR(384, 6, 256, 4)},
+       CLUSTERR(384, 6, 256, 4), CLUSTERR(384, 4, 384, 4)},
       {CLUSTER(512, 8, 256), LARGE(512), CLUSTER(512, 8, 512), CLUSTERR(512, 8, 256, 2),
        CLUSTERR(512, 8, 256, 4)},
   };
@@ -341,8 +341,8 @@ const std::vector<Variant>& variants(int b) {
 
 // Built-in shape per bin: the autotuner's choices on B200 (tuning.json), so a
 // caller that never runs the Python tuner (a C program, MATLAB) gets them too.
-const int kDefaultVariant[kNumBins] = {0, 0, 2, 5, 3, 6, 6, 4, 3};
-int g_variant[kNumBins] = {0, 0, 2, 5, 3, 6, 6, 4, 3};
+const int kDefaultVariant[kNumBins] = {0, 0, 2, 5, 3, 6, 6, 6, 3};
+int g_variant[kNumBins] = {0, 0, 2, 5, 3, 6, 6, 6, 3};
 
 int bin_of_k(int k) {
   for (int b = 0; b < kNumBins; ++b)
