@@ -37,6 +37,7 @@ import time
 import numpy as np
 
 import bench as B
+import workloads as W
 
 KV_C3 = (8, 16, 24, 32, 48, 64, 96, 128, 192, 256)
 
@@ -79,12 +80,10 @@ def run_c1(args):
     from paralanczos_b200 import api
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    m, n, k, nsets = 128, 512, 16, 10_000
-    rng = np.random.default_rng(B.SEED_PHI)
-    Phi = rng.standard_normal((m, n)) / np.sqrt(m)
-    A64 = Phi.T @ Phi
-    A32 = A64.astype(np.float32)
-    _, idx_h = O.gen_stream(B.SEED_SETS, 0, nsets, n, 0, k, k)
+    n, k, nsets = W.C1["n"], W.C1["k"], W.C1["nsets"]
+    A64, A32 = W.c1_matrix()
+    A64 = np.array(A64)
+    _, idx_h = api.gen_stream_host(B.SEED_SETS, 0, nsets, n, 0, k, k)
     idx_h = np.ascontiguousarray(idx_h, dtype=np.int32)
     eig = np.zeros(nsets * k)
     det = np.zeros(nsets)
@@ -97,7 +96,7 @@ def run_c1(args):
         assert rc == 0
     dropin_s = sum(t) / len(t)
     # device forms on the same sets
-    A = torch.from_numpy(A32).to(dev)
+    A = torch.from_numpy(np.array(A32)).to(dev)
     idx = torch.from_numpy(idx_h).to(dev)
     flush = torch.empty(256 << 18, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
@@ -110,7 +109,7 @@ def run_c1(args):
     worst = worst_all = 0.0
     for s in range(nsets):
         S = idx_h[s * k:(s + 1) * k]
-        w = O.dsyev_eigs(A64[np.ix_(S, S)])
+        w = B.dsyev_eigs(A64[np.ix_(S, S)])
         worst = max(worst, abs(lmin[s] - w[0]) / w[0], abs(lmax[s] - w[-1]) / w[-1])
         worst_all = max(worst_all, np.max(np.abs(eig[s * k:(s + 1) * k] - w)) / np.max(np.abs(w)))
     cpu = None
@@ -163,11 +162,8 @@ def run_c3(args):
     from paralanczos_b200._lib import lib
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    nsets, n = 300_000, B.N_COLS
-    gen = torch.Generator(device=dev).manual_seed(B.SEED_PHI)
-    Phi = torch.randn(B.M_ROWS, n, generator=gen, device=dev, dtype=torch.float64) / B.M_ROWS ** 0.5
-    A = (Phi.T @ Phi).to(torch.float32).contiguous()
-    del Phi
+    nsets, n = W.C3["nsets"], W.C3["n"]
+    A = torch.from_numpy(np.array(W.c2_matrix()[1])).to(dev)
     off_h, idx_h = api.gen_stream_host(B.SEED_SETS, 0, nsets, n, kdist=1)
     ks = np.diff(off_h)
     idx = torch.from_numpy(idx_h).to(dev)
@@ -193,7 +189,7 @@ def run_c3(args):
         worst = 0.0
         for s in sel:
             S = idx_h[off_h[s]:off_h[s + 1]]
-            w = O.dsyev_eigs(A64[np.ix_(S, S)])
+            w = B.dsyev_eigs(A64[np.ix_(S, S)])
             worst = max(worst, abs(lmin[s] - w[0]) / abs(w[0]), abs(lmax[s] - w[-1]) / abs(w[-1]))
         per_k[str(kv)] = {"sets": int(np.sum(ks == kv)), "checked": int(len(sel)), "max_rel_err": worst}
     # end to end through the C ABI with pinned host buffers
@@ -256,17 +252,12 @@ def run_c3(args):
 
 def _c4_frame(kind, dev):
     import torch
-    m, n = 2048, 16384
-    g = torch.Generator(device=dev).manual_seed(B.SEED_PHI)
-    if kind == "gauss":
-        return torch.randn(m, n, generator=g, device=dev, dtype=torch.float32) / m ** 0.5
-    return (torch.randint(0, 2, (m, n), generator=g, device=dev).float() * 2 - 1) / m ** 0.5
+    return torch.from_numpy(W.c4_frame("gauss" if kind == "gauss" else "rademacher")).to(dev)
 
 
 def _c4_accuracy(Phi, idx, out, k, nsample=2000):
     import torch
 
-    from oracle import oracle as O
     nsets = idx.numel() // k
     step = max(1, nsets // nsample)
     sel = torch.arange(0, nsets, step, device=Phi.device)[:nsample]
@@ -281,7 +272,7 @@ def _c4_accuracy(Phi, idx, out, k, nsample=2000):
         X = P64[:, Sc].permute(1, 0, 2)                      # (b, m, k)
         G = torch.bmm(X.transpose(1, 2), X).cpu().numpy()   # FP64 Gram of the FP32 frame
         for j in range(G.shape[0]):
-            w = O.dsyev_eigs(G[j])
+            w = B.dsyev_eigs(G[j])
             e = max(abs(lmin[c0 + j] - w[0]) / abs(w[0]), abs(lmax[c0 + j] - w[-1]) / abs(w[-1]))
             errs.append(e)
             worst = max(worst, e)
@@ -423,22 +414,12 @@ def run_c4(args):
 def _c5_matrices(dev):
     import torch
     out = []
-    specs = [("gauss", 1024, 4096), ("rad", 1024, 4096), ("gauss", 2048, 16384), ("corr", 1024, 4096)]
-    for i, (kind, m, n) in enumerate(specs):
-        g = torch.Generator(device=dev).manual_seed(100 + i)
-        if kind == "rad":
-            Phi = (torch.randint(0, 2, (m, n), generator=g, device=dev).double() * 2 - 1) / m ** 0.5
-        else:
-            Phi = torch.randn(m, n, generator=g, device=dev, dtype=torch.float64) / m ** 0.5
-        if kind == "corr":
-            # Phi (I + 0.3 T): column j gets 0.3 of its neighbours j-1 and j+1
-            P2 = Phi.clone()
-            P2[:, 1:] += 0.3 * Phi[:, :-1]
-            P2[:, :-1] += 0.3 * Phi[:, 1:]
-            Phi = P2
+    for label, m, n, kind, seed in W.C5_MATRICES:
+        # the frame from workloads.frame (host, seeded); its FP64 Gram on the GPU
+        Phi = torch.from_numpy(W.frame(m, n, seed, kind)).to(dev).double()
         A = (Phi.T @ Phi).to(torch.float32).contiguous()
         del Phi
-        out.append((f"{kind} {m}x{n}", A))
+        out.append((label, A))
         torch.cuda.synchronize()
     return out
 

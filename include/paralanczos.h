@@ -106,7 +106,9 @@ int pl_solve_host(const float *A, int n, long long lda, const int *idx, const lo
 
 /* The gather alone: blocks[s*k*k + i*k + j] = A[idx[s*k+i], idx[s*k+j]] (device
  * FP32, row-major blocks), err[s] (nullable) = PL_SET_BAD_INDEX for a set with
- * an index outside [0, n).  Uniform k <= PL_KMAX; asynchronous on `stream`.
+ * an index outside [0, n).  A is symmetric (as everywhere in this library):
+ * only the elements with i <= j are read, and each is written to (i, j) and
+ * (j, i).  Uniform k <= PL_KMAX; asynchronous on `stream`.
  * Replaces the reference's per-thread gather LOAD_SMS4H / LOAD_SMS4HF
  * (ParaLanczos.cu:455-490), which feeds its kernels' private strips.        */
 int pl_gather_blocks(const float *A, int n, long long lda, const int *idx, long long nsets, int k,
@@ -125,6 +127,15 @@ long long pl_gen_stream_host(unsigned long long seed, long long first, long long
 
 /* FP64 -> FP32 conversion on the device (for FP64 matrices). */
 int pl_convert_f64_f32(const double *in, float *out, long long count, void *stream);
+
+/* The drop-in entry points (calculate_subeigs*, calculate_eigs and their pl_*
+ * twins) keep the caller's FP64 matrix on the device, converted to FP32, and
+ * reuse it while later calls pass the same address, order and contents (a
+ * 64-bit content hash of the host matrix per call); the reference uploads it
+ * on every call (ParaLanczos.cu:1845-1846).  PL_DROPIN_CACHE=0 turns the
+ * reuse off.  Counts of reuses (hits) and uploads (misses) on the current
+ * device; either pointer may be NULL.                                        */
+void pl_dropin_cache_stats(long long *hits, long long *misses);
 
 /* ---- on-the-fly Gram form ------------------------------------------------
  * A is never materialised: each A[S,S] = Phi_S^T Phi_S is formed on the

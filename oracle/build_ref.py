@@ -12,7 +12,14 @@ extracted source is written under ``oracle/_ref/`` only, which is git-ignored:
 no reference source enters the repository.  Tests use the library to pin the
 oracle's own restatement (oracle/pl_oracle.c) bit-for-bit.
 
-Usage: python oracle/build_ref.py [--ref DIR]   (default DIR: /root/reference)
+It also compiles the reference's first example program (example1.cu, its
+caller of calculate_subeigs) against the reference's own ParaLanczos.h into
+``oracle/_ref/example1.o`` (object only), so a test can link that unchanged
+caller to libparalanczos_b200.so and run it.
+
+The reference tree is found at $PL_REFERENCE_DIR, else at the default below.
+
+Usage: python oracle/build_ref.py [--ref DIR]
 Exit status 0 also when the reference tree is absent (nothing to build).
 """
 from __future__ import annotations
@@ -20,11 +27,19 @@ from __future__ import annotations
 import argparse
 import os
 import re
+import shutil
 import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_ref")
+DEFAULT_REF = "/root/reference"
+
+
+def reference_dir() -> str | None:
+    """The reference tree ($PL_REFERENCE_DIR or the default), if present."""
+    d = os.environ.get("PL_REFERENCE_DIR") or DEFAULT_REF
+    return d if os.path.isfile(os.path.join(d, "ParaLanczos.cu")) else None
 
 
 def _cut_function(src: str, name: str) -> str:
@@ -90,12 +105,32 @@ def build(ref_dir: str) -> str | None:
     return so_path
 
 
+def build_example(ref_dir: str) -> str | None:
+    """example1.cu compiled, unchanged, against the reference's ParaLanczos.h."""
+    src = os.path.join(ref_dir, "example1.cu")
+    if not (os.path.isfile(src) and os.path.isfile(os.path.join(ref_dir, "ParaLanczos.h"))):
+        return None
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc):
+        return None
+    os.makedirs(OUT_DIR, exist_ok=True)
+    obj = os.path.join(OUT_DIR, "example1.o")
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-I", ref_dir, "-w", "-c", src,
+                    "-o", obj], check=True)
+    return obj
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None, help="reference tree (default: $PL_REFERENCE_DIR or the default)")
     a = ap.parse_args()
-    out = build(a.ref)
+    ref = a.ref or reference_dir()
+    out = build(ref) if ref else None
     print(out if out else "reference tree absent; nothing built")
+    if ref:
+        ex = build_example(ref)
+        if ex:
+            print(ex)
     return 0
 
 

@@ -33,6 +33,7 @@ SIGNATURES = {
     "pl_gather_blocks": (_i, [_vp, _i, _ll, _vp, _ll, _i, _vp, _vp, _vp]),
     "pl_gen_stream_host": (_ll, [C.c_ulonglong, _ll, _ll, _i, _i, _i, _i, _vp, _vp]),
     "pl_convert_f64_f32": (_i, [_vp, _vp, _ll, _vp]),
+    "pl_dropin_cache_stats": (None, [C.POINTER(_ll), C.POINTER(_ll)]),
     "pl_calculate_subeigs3": (_i, [_vp, _i, _i, _vp, _vp, _vp, _i]),
     "pl_calculate_subeigs": (_i, [_vp, _i, _vp, _vp, _vp, _i]),
     "pl_calculate_subeigs2": (_i, [_vp, _i, _i, _vp, _vp, _vp, _i]),

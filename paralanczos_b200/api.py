@@ -188,6 +188,16 @@ def gen_stream_host(seed: int, first: int, nsets: int, n: int, kdist: int = 0, k
     return offsets, idx
 
 
+def dropin_cache_stats() -> tuple[int, int]:
+    """(hits, misses) of the drop-in entry points' device matrix cache on the
+    current device: a hit reused the FP32 matrix already on the GPU, a miss
+    uploaded and converted the caller's FP64 matrix."""
+    import ctypes
+    h, m = ctypes.c_longlong(0), ctypes.c_longlong(0)
+    lib().pl_dropin_cache_stats(ctypes.byref(h), ctypes.byref(m))
+    return int(h.value), int(m.value)
+
+
 def fp32_peak(stream=None) -> float:
     """Measured FP32 FMA throughput of the current GPU in TFLOP/s."""
     import torch

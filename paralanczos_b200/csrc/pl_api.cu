@@ -14,6 +14,7 @@
 
 #include <mutex>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -384,10 +385,24 @@ struct DevScratch {
   size_t bytes = 0;
 };
 
+// The drop-in entry points' matrix, cached on the device between calls: the
+// caller's FP64 host matrix identified by its address, order and a content
+// hash, converted to FP32 on the device.
+struct MatCache {
+  const double* host = nullptr;
+  int n = 0;
+  uint64_t hash = 0;
+  bool valid = false;
+  long long hits = 0, misses = 0;
+};
+
 struct DevState {
   DevScratch large;    // k_large slots
   DevScratch bins;     // counts / starts / cursor / perm
   DevScratch upload;   // pl_solve_host and drop-in staging
+  DevScratch mat64;    // drop-in: the FP64 matrix as uploaded
+  DevScratch mat32;    // drop-in: its FP32 conversion (MatCache)
+  MatCache mc;
   cudaStream_t side[kNumBins] = {};
   cudaStream_t cap = nullptr;  // private stream the CSR graph is captured on
   cudaEvent_t ev_fork = nullptr;
@@ -652,6 +667,119 @@ int api_launch_binned(const MatrixF32& M, const int* idx, const long long* offse
 }
 void api_note_cuda(cudaError_t e) { g_last_cuda = (int)e; }
 int api_device_sms() { return device_sms(); }
+
+// 64-bit content hash of n doubles (their bit patterns), split over host
+// threads for large matrices: each chunk is a multiply-xorshift chain over its
+// words, the chunk hashes are combined in chunk order.
+static uint64_t mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+static uint64_t hash_chunk(const double* p, size_t n, uint64_t seed) {
+  uint64_t h = mix64(seed + n);
+  const uint64_t* w = reinterpret_cast<const uint64_t*>(p);
+  size_t i = 0;
+  for (; i + 4 <= n; i += 4) {  // four independent lanes, folded at the end
+    h = (h ^ mix64(w[i] + 0x9E3779B97F4A7C15ull)) * 0xff51afd7ed558ccdull;
+    h = (h ^ mix64(w[i + 1] + 0xC2B2AE3D27D4EB4Full)) * 0xc4ceb9fe1a85ec53ull;
+    h = (h ^ mix64(w[i + 2] + 0x165667B19E3779F9ull)) * 0xff51afd7ed558ccdull;
+    h = (h ^ mix64(w[i + 3] + 0x27D4EB2F165667C5ull)) * 0xc4ceb9fe1a85ec53ull;
+  }
+  for (; i < n; ++i) h = (h ^ mix64(w[i])) * 0xff51afd7ed558ccdull;
+  return mix64(h);
+}
+
+static uint64_t hash_doubles(const double* p, size_t n) {
+  const size_t kChunk = size_t(1) << 20;  // 8 MB per chunk
+  const size_t nchunks = (n + kChunk - 1) / kChunk;
+  std::vector<uint64_t> hs(nchunks ? nchunks : 1, 0);
+  unsigned nt = std::thread::hardware_concurrency();
+  nt = nt < 1 ? 1 : (nt > 16 ? 16 : nt);
+  if (nchunks < 2) nt = 1;
+  if (nt > nchunks) nt = (unsigned)nchunks;
+  auto work = [&](unsigned t) {
+    for (size_t c = t; c < nchunks; c += nt) {
+      const size_t b = c * kChunk, e = b + kChunk < n ? b + kChunk : n;
+      hs[c] = hash_chunk(p + b, e - b, c);
+    }
+  };
+  if (nt <= 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t) th.emplace_back(work, t);
+    for (auto& t : th) t.join();
+  }
+  uint64_t h = mix64(n);
+  for (uint64_t x : hs) h = mix64(h ^ x);
+  return h;
+}
+
+// The drop-in entry points' solve (ParaLanczos.cu:1811-1863 uploads the FP64
+// matrix on every call): the FP64 host matrix is uploaded and converted to
+// FP32 on the device once, and reused while the caller passes the same
+// address, order and contents (PL_DROPIN_CACHE=0 re-uploads every call); the
+// index sets go up, all k eigenvalues and the determinants (and per-set
+// status) come back.  Synchronous on the legacy default stream, like the
+// reference.
+int api_solve_f64_host(const double* mat, int n, const int* subIndex, long long nsets, int k, int form,
+                       double* eig, double* det, int* err) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!mat || !subIndex || n <= 0 || nsets < 0 || k < 1 || k > n) return PL_EINVAL;
+  if (nsets == 0) return PL_OK;
+  DevState& d = state();
+  cudaStream_t st = 0;
+  const size_t nn = (size_t)n * (size_t)n;
+  static const bool cache_on = env_flag("PL_DROPIN_CACHE", true);
+  const uint64_t h = cache_on ? hash_doubles(mat, nn) : 0;
+  if (!(cache_on && d.mc.valid && d.mc.host == mat && d.mc.n == n && d.mc.hash == h)) {
+    d.mc.valid = false;
+    int rc = ensure(d.mat64, sizeof(double) * nn);
+    if (rc) return rc;
+    rc = ensure(d.mat32, sizeof(float) * nn);
+    if (rc) return rc;
+    PL_CU(cudaMemcpyAsync(d.mat64.p, mat, sizeof(double) * nn, cudaMemcpyHostToDevice, st));
+    const long long g = ((long long)nn + 255) / 256;
+    k_f64_to_f32<<<(unsigned)(g < 8192 ? g : 8192), 256, 0, st>>>((const double*)d.mat64.p, (float*)d.mat32.p,
+                                                                (long long)nn);
+    PL_CU(cudaGetLastError());
+    d.mc.host = mat;
+    d.mc.n = n;
+    d.mc.hash = h;
+    d.mc.valid = cache_on;
+    ++d.mc.misses;
+  } else {
+    ++d.mc.hits;
+  }
+  const long long total = nsets * (long long)k;
+  const size_t bytes = align256(sizeof(int) * total) + align256(sizeof(double) * total) +
+                       align256(sizeof(double) * nsets) + align256(sizeof(int) * nsets) + 1024;
+  int rc = ensure(d.upload, bytes);
+  if (rc) return rc;
+  Carve cv{(char*)d.upload.p, 0};
+  int* dI = cv.take<int>(total);
+  double* deig = cv.take<double>(total);
+  double* ddet = cv.take<double>(nsets);
+  int* derr = cv.take<int>(nsets);
+  PL_CU(cudaMemcpyAsync(dI, subIndex, sizeof(int) * total, cudaMemcpyHostToDevice, st));
+  SetOutputs out{nullptr, nullptr, nullptr, derr, deig, ddet};
+  rc = solve_dev((const float*)d.mat32.p, n, n, dI, nullptr, nsets, k, form, out, st);
+  if (rc) return rc;
+  if (eig) PL_CU(cudaMemcpyAsync(eig, deig, sizeof(double) * total, cudaMemcpyDeviceToHost, st));
+  if (det) PL_CU(cudaMemcpyAsync(det, ddet, sizeof(double) * nsets, cudaMemcpyDeviceToHost, st));
+  if (err) PL_CU(cudaMemcpyAsync(err, derr, sizeof(int) * nsets, cudaMemcpyDeviceToHost, st));
+  PL_CU(cudaStreamSynchronize(st));
+  return PL_OK;
+}
+
+void api_dropin_cache_stats(long long* hits, long long* misses) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  const DevState& d = state();
+  if (hits) *hits = d.mc.hits;
+  if (misses) *misses = d.mc.misses;
+}
 }  // namespace pl
 
 // =============================================================================
@@ -824,6 +952,8 @@ int pl_convert_f64_f32(const double* in, float* out, long long count, void* stre
   return PL_OK;
 }
 
+void pl_dropin_cache_stats(long long* hits, long long* misses) { api_dropin_cache_stats(hits, misses); }
+
 int pl_tune_set(int bin, int variant) {
   std::lock_guard<std::mutex> lk(g_mu);
   if (bin < 0 || bin >= kNumBins) return PL_EINVAL;
@@ -877,11 +1007,12 @@ int pl_release(void) {
   DevState& d = state();
   for (auto& kv : d.graphs) cudaGraphExecDestroy(kv.second.exec);
   d.graphs.clear();
-  for (DevScratch* s : {&d.large, &d.bins, &d.upload}) {
+  for (DevScratch* s : {&d.large, &d.bins, &d.upload, &d.mat64, &d.mat32}) {
     if (s->p) cudaFree(s->p);
     s->p = nullptr;
     s->bytes = 0;
   }
+  d.mc.valid = false;
   gram_release();
   return PL_OK;
 }

@@ -6,10 +6,13 @@
 // deliberately different:
 //   * no cudaDeviceReset (ParaLanczos.cu:1700/1717, 1739/1760, 1783/1803,
 //     1837/1858): the caller's CUDA context survives;
-//   * the FP64 input is converted to FP32 on the device and solved by the
-//     batched engine (full reorthogonalisation, all k eigenvalues by FP64
-//     bisection); Det is the product of the eigenvalues (the reference's KER
-//     path evaluates DET_TRIDIAG over the full matrix order, ParaLanczos.cu:1138);
+//   * the FP64 input is uploaded, converted to FP32 on the device and kept
+//     there while later calls pass the same matrix (address, order and a
+//     content hash; the reference re-uploads it every call,
+//     ParaLanczos.cu:1845-1846), then solved by the batched engine (full
+//     reorthogonalisation, all k eigenvalues by FP64 bisection); Det is the
+//     product of the eigenvalues (the reference's KER path evaluates
+//     DET_TRIDIAG over the full matrix order, ParaLanczos.cu:1138);
 //   * calculate_subeigs3 solves every subIndexLen/subn set (the reference's
 //     grid of subIndexLen/128 blocks skips a ragged tail, ParaLanczos.cu:1829);
 //   * stdout lines of the reference only with PL_VERBOSE=1;
@@ -23,6 +26,7 @@
 #include <vector>
 
 #include "../../include/paralanczos.h"
+#include "pl_internal.h"
 
 namespace {
 
@@ -32,22 +36,12 @@ bool env_on(const char* name, bool dflt) {
   return !(v[0] == '0' || v[0] == 'n' || v[0] == 'N' || v[0] == 'f' || v[0] == 'F');
 }
 
-// All-eigenvalue solve of nsets uniform-k sets of an FP64 host matrix.
+// All-eigenvalue solve of nsets uniform-k sets of an FP64 host matrix: the
+// matrix is uploaded and converted to FP32 on the device, and kept there
+// while later calls pass the same matrix (pl_api.cu, api_solve_f64_host).
 int solve_f64_host(const double* mat, int n, const int* subIndex, int nsets, int k, int form,
                    double* eig, double* det, int* err) {
-  const size_t nn = (size_t)n * n;
-  std::vector<float> A32(nn);
-  for (size_t i = 0; i < nn; ++i) A32[i] = (float)mat[i];
-  std::vector<double> detv(nsets);
-  std::vector<int> errv(nsets);
-  int rc = pl_solve_host(A32.data(), n, n, subIndex, nullptr, nsets, k, form, nullptr, nullptr,
-                         nullptr, errv.data(), eig, detv.data());
-  if (rc) return rc;
-  if (det)
-    for (int s = 0; s < nsets; ++s) det[s] = detv[s];
-  if (err)
-    for (int s = 0; s < nsets; ++s) err[s] = errv[s];
-  return PL_OK;
+  return pl::api_solve_f64_host(mat, n, subIndex, nsets, k, form, eig, det, err);
 }
 
 }  // namespace

@@ -40,4 +40,13 @@ int api_device_sms();
 // Frees the Gram form's cached device buffers (called by pl_release).
 void gram_release();
 
+// The drop-in entry points' solve of nsets uniform-k sets of an FP64 host
+// matrix (n x n): the matrix is cached on the device (FP32) between calls with
+// the same address, order and contents; all k eigenvalues, det and err out.
+int api_solve_f64_host(const double* mat, int n, const int* subIndex, long long nsets, int k, int form,
+                       double* eig, double* det, int* err);
+
+// Hits and misses of the drop-in matrix cache on the current device.
+void api_dropin_cache_stats(long long* hits, long long* misses);
+
 }  // namespace pl

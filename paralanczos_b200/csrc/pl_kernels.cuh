@@ -344,34 +344,97 @@ __global__ void k_f64_to_f32(const double* __restrict__ in, float* __restrict__ 
 
 // The gather on its own: block s of `blocks` (k x k, row-major) = A[S_s, S_s]
 // (LOAD_SMS4H / LOAD_SMS4HF, ParaLanczos.cu:455-490, without the per-thread
-// 4x4 strips).  One set per block at a time: the set's indices go to shared
-// memory, then every thread copies elements with consecutive output
-// addresses, so the writes are coalesced and all reads of a set are in
-// flight together.  err[s] = SET_BAD_INDEX for an index outside [0, n) (its
-// block is left as zeros).
+// 4x4 strips).  A is symmetric, so only the elements A[S_i, S_j] with i <= j
+// are read (k(k+1)/2 random 4-byte loads per set: each one is its own L1
+// request and 32-byte sector, the cost of a random gather) and each is
+// written to (i, j) and (j, i).  One set per CTA at a time, in 64 x 64 tiles
+// (I <= J): a diagonal tile is read as its upper triangle and mirrored in
+// shared memory; an off-diagonal tile is read whole, written as tile (I, J)
+// straight from registers and as tile (J, I) through a shared-memory
+// transpose.  Warp w of the 8 owns tile rows w, w + 8, ...; lane l columns
+// l and l + 32; every load of a tile is issued before the first is used, and
+// every global write is a coalesced 128-byte row segment.  err[s] =
+// SET_BAD_INDEX for an index outside [0, n) (its block is left as zeros).
+constexpr int kGTile = 64, kGRows = kGTile / 8;
+
+__device__ __forceinline__ void gather_tile(const float* __restrict__ A, long long lda, const int* sidx, int k,
+                                            int I, int J, float* __restrict__ out, float (*T)[kGTile + 1]) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r0 = I * kGTile, c0 = J * kGTile;
+  const bool diag = I == J;
+  float e[kGRows][2];
+#pragma unroll
+  for (int u = 0; u < kGRows; ++u) {
+    const int r = w + 8 * u;
+    const bool rv = r0 + r < k;
+    const float* __restrict__ row = A + (size_t)sidx[rv ? r0 + r : 0] * (size_t)lda;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int c = lane + 32 * h;
+      const bool v = rv && c0 + c < k && (!diag || c >= r);
+      e[u][h] = v ? __ldg(row + sidx[c0 + c]) : 0.f;
+    }
+  }
+  if (diag) {
+#pragma unroll
+    for (int u = 0; u < kGRows; ++u) {
+      const int r = w + 8 * u;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int c = lane + 32 * h;
+        if (c >= r) {
+          T[r][c] = e[u][h];
+          T[c][r] = e[u][h];
+        }
+      }
+    }
+  } else {
+#pragma unroll
+    for (int u = 0; u < kGRows; ++u) {
+      const int r = w + 8 * u;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int c = lane + 32 * h;
+        T[c][r] = e[u][h];
+        if (r0 + r < k && c0 + c < k) out[(size_t)(r0 + r) * k + c0 + c] = e[u][h];
+      }
+    }
+  }
+  __syncthreads();
+  // tile (J, I) from the transpose buffer (for a diagonal tile: (I, I) whole)
+#pragma unroll
+  for (int u = 0; u < kGRows; ++u) {
+    const int r = w + 8 * u;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int c = lane + 32 * h;
+      if (c0 + r < k && r0 + c < k) out[(size_t)(c0 + r) * k + r0 + c] = T[r][c];
+    }
+  }
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(256) k_gather_blocks(const float* __restrict__ A, int n, long long lda,
                                                       const int* __restrict__ idx, long long nsets, int k,
                                                       float* __restrict__ blocks, int* __restrict__ err) {
   __shared__ int sidx[512];
-  __shared__ int bad;
+  __shared__ float T[kGTile][kGTile + 1];
   const long long kk = (long long)k * k;
+  const int nt = (k + kGTile - 1) / kGTile;
   for (long long s = blockIdx.x; s < nsets; s += gridDim.x) {
-    if (threadIdx.x == 0) bad = 0;
-    __syncthreads();
+    int bad = 0;
     for (int c = threadIdx.x; c < k; c += blockDim.x) {
       const int v = __ldg(idx + s * k + c);
-      if (v < 0 || v >= n) bad = 1;
+      bad |= (v < 0) | (v >= n);
       sidx[c] = v;
     }
-    __syncthreads();
+    bad = __syncthreads_or(bad);
     float* __restrict__ out = blocks + s * kk;
     if (bad) {
       for (long long e = threadIdx.x; e < kk; e += blockDim.x) out[e] = 0.f;
     } else {
-      for (long long e = threadIdx.x; e < kk; e += blockDim.x) {
-        const int r = (int)(e / k), c = (int)(e - (long long)r * k);
-        out[e] = __ldg(A + (size_t)sidx[r] * (size_t)lda + sidx[c]);
-      }
+      for (int I = 0; I < nt; ++I)
+        for (int J = I; J < nt; ++J) gather_tile(A, lda, sidx, k, I, J, out, T);
     }
     if (threadIdx.x == 0 && err) err[s] = bad ? SET_BAD_INDEX : SET_OK;
     __syncthreads();

@@ -4,13 +4,14 @@ Each case builds its inputs on the GPU, runs the kernel once to warm up
 (module load, scratch allocation) and then `--launches` more times, so a
 profiler can skip the first launch and capture the next ones:
 
-    python -m paralanczos_b200.profile_case --case k64 [--nsets 200000]
+    python profile_case.py --case k64 [--nsets 200000]
     ncu --set full --clock-control none -k regex:k_sa_solve -s 1 -c 1 \\
-        python -m paralanczos_b200.profile_case --case k64
+        python profile_case.py --case k64
 
 Cases:
-  k64      batched form, k = 64, A = Phi^T Phi (Phi 1024 x 4096 N(0, 1/1024)),
-           sets from the counter-based generator (seed 1); the tuned variant.
+  k64      batched form, k = 64, A = Phi^T Phi (Phi 1024 x 4096 N(0, 1/1024),
+           workloads.c2_matrix), sets from the counter-based generator
+           (seed 1); the tuned variant.
   plain64  the same sets through the one-set-per-block form.
   k128     batched form, k = 128 on the same matrix.
   k192     batched form, k = 192 (one-SM engine of the cluster kernel).
@@ -21,8 +22,11 @@ Cases:
 from __future__ import annotations
 
 import argparse
+import os
 import sys
 import time
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 
 
 def main(argv=None) -> int:
@@ -34,30 +38,29 @@ def main(argv=None) -> int:
     ap.add_argument("--variant", type=int, default=-2,
                     help="kernel variant of the case's k bin (pl_tune_describe); default: the tuned one")
     a = ap.parse_args(argv)
+    import numpy as np
     import torch
 
-    from . import api
+    import workloads as W
+    from paralanczos_b200 import api
     if a.variant >= -1:
         kb = {"k64": 64, "plain64": 64, "k128": 128, "k192": 192, "k256": 256, "gram": 128, "uneven": 0}[a.case]
         b = next(i for i in range(api.num_bins()) if api.bin_kmax(i) >= kb) if kb else 0
         api.tune_set(b, a.variant)
         print(f"bin {b}: variant {a.variant} ({api.tune_describe(b, max(a.variant, 0))[1]})")
     dev = torch.device("cuda", 0)
-    g = torch.Generator(device=dev).manual_seed(0)
     t0 = time.perf_counter()
     if a.case == "gram":
-        m, n, k = 2048, 16384, 128
+        n, k = W.C4["n"], W.C4["k"]
         nsets = a.nsets or 8192
-        Phi = torch.randn(m, n, generator=g, device=dev, dtype=torch.float32) / m ** 0.5
+        Phi = torch.from_numpy(W.c4_frame("gauss")).to(dev)
         gf = api.GramFrame(Phi)
         idx = api.gen_sets(1, 0, nsets, n, k)
         for _ in range(1 + a.launches):
             gf.blocks(idx, k)
     else:
-        m, n = 1024, 4096
-        Phi = torch.randn(m, n, generator=g, device=dev, dtype=torch.float64) / m ** 0.5
-        A = (Phi.T @ Phi).to(torch.float32).contiguous()
-        del Phi
+        n = W.C2["n"]
+        A = torch.from_numpy(np.array(W.c2_matrix()[1])).to(dev)
         if a.case == "uneven":
             nsets = a.nsets or 100_000
             off_h, idx_h = api.gen_stream_host(1, 0, nsets, n, kdist=1)

@@ -86,3 +86,23 @@ def test_dropin_reference_validation_messages(capfd):
     assert "'int subn' must be divisible by 4" in capfd.readouterr().err
     assert api.calculate_subeigs3(mat, 120, 8, eig, det, sub, 4) == _lib.PL_EINVAL
     assert "'subIndexLen' must be divisible by 32" in capfd.readouterr().err
+
+
+def test_reference_example1_object_links(tmp_path):
+    """The reference's example1.cu, compiled against the reference's own
+    ParaLanczos.h (oracle/_ref/example1.o, built when the reference tree is
+    present), resolves every symbol it needs from libparalanczos_b200.so."""
+    import shutil
+
+    import pytest
+    obj = os.path.join(ROOT, "oracle", "_ref", "example1.o")
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(obj) or not os.path.exists(nvcc):
+        pytest.skip("reference example1 object or nvcc absent")
+    _lib.lib()
+    libdir = os.path.dirname(_lib.LIB_PATH)
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", obj, "-o", str(tmp_path / "example1"),
+                    "-L", libdir, "-lparalanczos_b200", "-Xlinker", f"-rpath={libdir}"], check=True,
+                   capture_output=True, text=True, timeout=300)
+    undef = subprocess.run(["nm", "-u", obj], capture_output=True, text=True, check=True).stdout
+    assert "_Z17calculate_subeigsPdiS_S_Pii" in undef

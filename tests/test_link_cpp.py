@@ -2,10 +2,11 @@
 
 The reference's examples include ParaLanczos.h and call calculate_subeigs3 /
 calculate_eigs with C++ linkage (their objects reference
-_Z18calculate_subeigs3PdiiS_S_Pii).  This test compiles a small C++ program of
-its own against include/ParaLanczos.h, links it to libparalanczos_b200.so with
-no other change, runs it on the GPU and checks the printed eigenvalues and
-determinants against LAPACK dsyev.
+_Z18calculate_subeigs3PdiiS_S_Pii).  These tests link such callers to
+libparalanczos_b200.so with no other change, run them on the GPU and check
+the eigenvalues and determinants against LAPACK dsyev: a small C++ program of
+this project compiled against include/ParaLanczos.h, and the reference's own
+example1.cu compiled unchanged against the reference's header.
 """
 import os
 import shutil
@@ -85,3 +86,43 @@ def test_cpp_program_links_and_runs(tmp_path):
     w = O.dsyev_eigs(A)
     assert np.max(np.abs(np.array(vals["F"]) - w)) <= 1e-5 * np.max(np.abs(w))
     assert abs(vals["G"][0] - np.prod(w)) <= 1e-4 * abs(np.prod(w))
+
+
+EXAMPLE1_OBJ = os.path.join(ROOT, "oracle", "_ref", "example1.o")
+
+
+def _link_example1(tmp_path):
+    """The reference's own example1.cu, compiled unchanged against the
+    reference's ParaLanczos.h at build time (oracle/build_ref.py writes
+    oracle/_ref/example1.o), linked to libparalanczos_b200.so."""
+    from paralanczos_b200 import _lib
+    _lib.lib()
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    libdir = os.path.join(ROOT, "paralanczos_b200")
+    exe = tmp_path / "example1"
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", EXAMPLE1_OBJ, "-o", str(exe), "-L", libdir,
+                    "-lparalanczos_b200", "-Xlinker", f"-rpath={libdir}"], check=True, capture_output=True,
+                   text=True, timeout=300)
+    return exe
+
+
+@pytest.mark.skipif(not os.path.exists(EXAMPLE1_OBJ), reason="reference example1 object not built")
+def test_reference_example1_runs_against_the_library(tmp_path):
+    """example1.cu (ParaLanczos example1.cu:14-54): calculate_subeigs on its 8 x 8
+    matrix (example1.cu:19-26) with the subset {1, 3, 5, 7} (example1.cu:39-42).
+    It allocates Eigenvalues[8] and one Det, enough for the 4 eigenvalues and the
+    determinant the call writes.  With PL_VERBOSE=1 the library prints the
+    reference's "%d eigenvalue: %g" lines, checked against dsyev."""
+    import json
+
+    from oracle import oracle as O
+    exe = _link_example1(tmp_path)
+    env = dict(os.environ, PL_VERBOSE="1")
+    r = subprocess.run([str(exe)], check=True, capture_output=True, text=True, timeout=120, env=env)
+    got = [float(line.split(":")[1]) for line in r.stdout.splitlines() if "eigenvalue:" in line]
+    fx = json.load(open(os.path.join(ROOT, "tests", "golden", "fixture8.json")))
+    g = np.array(fx["matrix"]).reshape(8, 8)
+    w = O.dsyev_eigs(g[np.ix_([1, 3, 5, 7], [1, 3, 5, 7])])
+    assert len(got) == 4, r.stdout
+    # %g prints six significant digits
+    np.testing.assert_allclose(got, w, rtol=1e-5)
