@@ -372,6 +372,8 @@ def run_ours(args):
     del gout
     g_read = gsets * (4.0 * K * (K + 1) / 2 + 4.0 * K) / g_s / 1e9
     g_write = gsets * 4.0 * K * K / g_s / 1e9
+    g_elems = gsets * K * (K + 1) / 2 / g_s / 1e9          # random elements, G/s
+    g_ceiling = api.gather_peak()                          # measured random-load ceiling, G/s
 
     peak_fp32 = api.fp32_peak()
     peaks, peak_src = measured_peaks()
@@ -416,6 +418,10 @@ def run_ours(args):
                                 "algorithmic": "4k(k+1)/2 + 4k + 28 bytes per set over the whole kernel"},
             "gather_only": {"sets": gsets, "ms": g_s * 1e3, "read_gbs": g_read, "write_gbs": g_write,
                             "frac_hbm": (g_read + g_write) / peaks.get("hbm_gbs"),
+                            "random_gelems": g_elems, "ceiling_gelems": g_ceiling,
+                            "frac_ceiling": g_elems / g_ceiling,
+                            "ceiling": "uniformly random 4-byte loads from an L2-resident array, measured "
+                                       "live (pl_gather_peak): each element is its own L1 request and sector",
                             "kernel": "k_gather_blocks (pl_gather_blocks): A[S,S] written as k x k blocks",
                             "algorithmic": "read 4k(k+1)/2 + 4k bytes, write 4k^2 bytes per set"},
             "clocks": sampler.summary(),

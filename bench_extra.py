@@ -548,7 +548,9 @@ def run_c5(args):
                 "served": {"p50_ms": 1e3 * _pct(lat, 50), "p99_ms": 1e3 * _pct(lat, 99),
                            "server_p50_ms": 1e3 * st["p50_s"], "server_p99_ms": 1e3 * st["p99_s"],
                            "solves_s": sets / span, "waves": int(st["waves"]),
-                           "waves_inflight_max": int(st["waves_inflight_max"]),
+                           "loops_running_max": int(st["loops_running_max"]),
+                           "loop_launches": int(st["loop_launches"]), "idle_exits": int(st["idle_exits"]),
+                           "device_mb": st["device_bytes"] / 2 ** 20,
                            "arena_peak_mb": st["arena_peak"] / 2 ** 20},
                 "plain_per_call": {"p50_ms": 1e3 * _pct(lat_p, 50), "p99_ms": 1e3 * _pct(lat_p, 99),
                                    "solves_s": sets / span_p}})

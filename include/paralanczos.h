@@ -167,16 +167,22 @@ int pl_solve_gram(const void *prep, int m, int n, const int *idx, long long nset
  * No counterpart in the reference (each calculate_subeigs* call is one
  * synchronous batch on one matrix, ParaLanczos.cu:1725-1863).  A server keeps
  * matrices resident and solves requests (matrix, k, nsets index sets) as they
- * arrive: a scheduler thread admits queued requests in arrival order while
- * their indices fit `budget_bytes` of HBM, and runs the admitted work in
- * waves of about PL_SERVE_WAVE_MS (default 20) ms of GPU work -- sets of any
- * matrix and k, binned by k on the device; the oldest unfinished request
- * takes up to PL_SERVE_OLDEST_SHARE (default 0.9) of each wave and the rest
- * goes to the requests with the least work left, so large requests are split
- * over waves and small ones go first -- with up to `max_waves` waves in
- * flight on their own streams.  Extremes only (lambda_min, lambda_max,
- * delta_k, err).
- * Host buffers; thread-safe.                                                 */
+ * arrive.  The host admits queued requests in arrival order while their
+ * indices fit the server's arena, uploads them and publishes a descriptor per
+ * request into a ring in mapped host memory; the batching itself runs on the
+ * GPU in up to `max_waves` (at most 4) device-resident request loops, one
+ * CUDA graph each (a conditional WHILE node over: plan, expand, binned solve,
+ * finish), requests spread over the loops by k.  Each pass a loop forms a
+ * wave of about PL_SERVE_WAVE_MS (default 20) ms of GPU work -- the oldest
+ * unfinished request takes up to PL_SERVE_OLDEST_SHARE (default 0.9) of it,
+ * the requests with the least work left the rest, so large requests are split
+ * over waves and small ones go first -- and writes results and completion
+ * flags straight into mapped host memory.  A loop with no work waits at most
+ * PL_SERVE_IDLE_MS (default 20) on the device and ends; the next request
+ * launches it again.  `budget_bytes` bounds ALL device memory of the server
+ * (loop staging and kernel scratch first, the rest is the index arena);
+ * PL_EINVAL if it does not exceed the staging by at least 1 MiB.  Extremes
+ * only (lambda_min, lambda_max, delta_k, err).  Host buffers; thread-safe.    */
 /* `host_pool_bytes` of pinned memory stage submitted indices and results.    */
 int pl_serve_create(long long budget_bytes, long long host_pool_bytes, int max_waves, void **server);
 /* Register a device-resident symmetric FP32 matrix (kept by reference: it must
@@ -192,12 +198,13 @@ int pl_serve_submit(void *server, int matrix_id, const int *idx, long long nsets
  * forgets the request.  PL_ETIMEDOUT: not finished yet (still queued).       */
 int pl_serve_wait(void *server, long long request_id, double timeout_s, double *lmin, double *lmax,
                   double *delta, int *err, double *latency_s);
-/* out[0..11]: completed requests, sets solved, p50, p99, mean and max latency
+/* out[0..15]: completed requests, sets solved, p50, p99, mean and max latency
  * (s), busy span first admission .. last completion (s), peak and total arena
- * bytes, waves launched, most waves in flight at once, requests queued.      */
+ * bytes, waves formed, most loops running at once, requests queued, loop
+ * launches, loops ended idle, device bytes held by the server, loops running. */
 int pl_serve_stats(void *server, double *out, int nout);
 int pl_serve_reset_stats(void *server);
-/* Stops the scheduler (in-flight waves finish first) and frees everything.  */
+/* Stops the loops (a wave in progress finishes first) and frees everything.  */
 int pl_serve_destroy(void *server);
 
 /* ---- ParaLanczos.h drop-ins with a status return ------------------------ */
@@ -238,6 +245,10 @@ int pl_num_bins(void);
 int pl_bin_kmax(int bin);
 /* Measured FP32 FMA throughput of this GPU (TFLOP/s), for roofline figures. */
 int pl_fp32_peak(double *tflops, void *stream);
+/* Measured rate of uniformly random 4-byte loads from an L2-resident array
+ * (G elements/s): the ceiling of the A[S,S] gather, whose every element is
+ * its own 32-byte sector.  Allocates and frees a 64 MiB buffer.              */
+int pl_gather_peak(double *gelems, void *stream);
 /* Releases cached device scratch, graphs and streams of this library. */
 int pl_release(void);
 

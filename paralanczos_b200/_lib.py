@@ -43,6 +43,7 @@ SIGNATURES = {
     "pl_num_bins": (_i, []),
     "pl_bin_kmax": (_i, [_i]),
     "pl_fp32_peak": (_i, [C.POINTER(_d), _vp]),
+    "pl_gather_peak": (_i, [C.POINTER(_d), _vp]),
     "pl_release": (_i, []),
     "pl_gram_prep_bytes": (_ll, [_i, _i]),
     "pl_gram_prepare": (_i, [_vp, _ll, _i, _i, _vp, _vp]),

@@ -207,6 +207,16 @@ def fp32_peak(stream=None) -> float:
     return v.value
 
 
+def gather_peak(stream=None) -> float:
+    """Measured rate of uniformly random 4-byte loads from an L2-resident array
+    (G elements/s): the ceiling of the A[S,S] gather."""
+    import torch
+    st = stream if stream is not None else torch.cuda.current_stream()
+    v = C.c_double(0.0)
+    check(lib().pl_gather_peak(C.byref(v), st.cuda_stream), "pl_gather_peak")
+    return v.value
+
+
 def num_bins() -> int:
     return lib().pl_num_bins()
 
@@ -285,12 +295,16 @@ class GramFrame:
 # --------------------------------------------------------------------------- serving
 
 SERVE_STATS = ("completed", "sets", "p50_s", "p99_s", "mean_s", "max_s", "busy_s", "arena_peak",
-               "arena_bytes", "waves", "waves_inflight_max", "queued")
+               "arena_bytes", "waves", "loops_running_max", "queued", "loop_launches", "idle_exits",
+               "device_bytes", "loops_running")
 
 
 class Server:
     """Continuous-batching server over device-resident matrices (pl_serve_*).
 
+    Requests are batched on the GPU by device-resident request loops (one
+    CUDA graph each, ``max_waves`` of them, requests spread over them by k);
+    all of the server's device memory lies within ``budget_bytes``.
     ``submit`` queues a request and returns its id (raises PLError with status
     PL_EBUSY when the pinned pool is full); ``wait`` returns its results as a
     dict of numpy arrays plus ``latency_s`` (submit to completion)."""

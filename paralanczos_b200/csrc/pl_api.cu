@@ -233,10 +233,10 @@ cudaError_t launch_large(const MatrixF32& M, const SetSource& src, const SetOutp
   return cudaGetLastError();
 }
 
-template <int KB, int CS, int NTC, int RPT = 1>
+template <int KB, int CS, int NTC, int RPT = 1, bool SPLIT = false>
 cudaError_t launch_cluster(const MatrixF32& M, const SetSource& src, const SetOutputs& out,
                            long long nitems, void*, cudaStream_t st, bool prep) {
-  auto kern = k_cluster_solve<KB, CS, NTC, RPT>;
+  auto kern = k_cluster_solve<KB, CS, NTC, RPT, SPLIT>;
   const size_t dsm = sizeof(ClusterSmem<KB, CS, NTC>);
   static int maxcl = [&] {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
@@ -311,6 +311,13 @@ struct Variant {
     "cluster KB=" #KB " CS=" #CS " NTC=" #NTC " RPT=" #RPT,                                     \
         {launch_cluster<KB, CS, NTC, RPT>, nullptr}, {scratch_none, scratch_none}               \
   }
+// the same with each per-step cluster exchange split into arrive ... wait
+// around independent work (cluster_solve_set_split)
+#define CLUSTERS(KB, CS, NTC, RPT)                                                            \
+  Variant {                                                                                     \
+    "cluster split KB=" #KB " CS=" #CS " NTC=" #NTC " RPT=" #RPT,                               \
+        {launch_cluster<KB, CS, NTC, RPT, true>, nullptr}, {scratch_none, scratch_none}         \
+  }
 #define LARGE(KM) \
   Variant {                                                                             \
     "large KM=" #KM " CTA=256", {launch_large<KM, false>, launch_large<KM, true>},      \
@@ -331,11 +338,13 @@ const std::vector<Variant>& variants(int b) {
       {CLUSTER(192, 2, 384), LARGE(256), CLUSTER(192, 4, 192), CLUSTER(192, 1, 384), CLUSTER(192, 1, 768),
        CLUSTERR(192, 1, 384, 2), CLUSTERR(192, 1, 384, 4)},
       {CLUSTER(256, 2, 512), LARGE(256), CLUSTER(256, 4, 256), CLUSTER(256, 8, 256), CLUSTER(256, 2, 256),
-       CLUSTERR(256, 2, 256, 2), CLUSTERR(256, 2, 256, 4)},
+       CLUSTERR(256, 2, 256, 2), CLUSTERR(256, 2, 256, 4), CLUSTERS(256, 2, 256, 4), CLUSTERS(256, 2, 256, 2),
+       CLUSTERS(256, 4, 256, 2)},
       {CLUSTER(384, 4, 384), LARGE(512), CLUSTER(384, 8, 192), CLUSTER(384, 6, 256), CLUSTERR(384, 6, 256, 2),
-       CLUSTERR(384, 6, 256, 4), CLUSTERR(384, 4, 384, 4)},
+       CLUSTERR(384, 6, 256, 4), CLUSTERR(384, 4, 384, 4), CLUSTERS(384, 4, 384, 4),
+       CLUSTERS(384, 6, 256, 2)},
       {CLUSTER(512, 8, 256), LARGE(512), CLUSTER(512, 8, 512), CLUSTERR(512, 8, 256, 2),
-       CLUSTERR(512, 8, 256, 4)},
+       CLUSTERR(512, 8, 256, 4), CLUSTERS(512, 8, 256, 2), CLUSTERS(512, 8, 256, 4)},
   };
   return v[b];
 }
@@ -510,7 +519,7 @@ cudaError_t enqueue_binned(const MatrixF32& M, const int* idx, const long long* 
                            long long nsets, const SetOutputs& out, const LaunchFn fns[kNumBins],
                            int* hdr, char* qscratch, const size_t qoff[kNumBins], cudaStream_t cs,
                            const cudaStream_t side[kNumBins], cudaEvent_t fork,
-                           const cudaEvent_t join[kNumBins]) {
+                           const cudaEvent_t join[kNumBins], const long long* nsets_dev = nullptr) {
   const int nb = kNumBins;
   int* counts = hdr;
   int* starts = hdr + 16;
@@ -527,11 +536,11 @@ cudaError_t enqueue_binned(const MatrixF32& M, const int* idx, const long long* 
   const int tb = 256;
   const long long g = (nsets + tb - 1) / tb;
   const unsigned grid = (unsigned)(g < 4096 ? (g > 0 ? g : 1) : 4096);
-  k_bin_count<<<grid, tb, 0, cs>>>(offsets, nsets, bt, counts);
+  k_bin_count<<<grid, tb, 0, cs>>>(offsets, nsets, bt, counts, nsets_dev);
   note(cudaGetLastError());
   k_bin_scan<<<1, 32, 0, cs>>>(counts, nb, starts, cursor);
   note(cudaGetLastError());
-  k_bin_scatter<<<grid, tb, 0, cs>>>(offsets, nsets, bt, starts, cursor, perm);
+  k_bin_scatter<<<grid, tb, 0, cs>>>(offsets, nsets, bt, starts, cursor, perm, nsets_dev);
   note(cudaGetLastError());
   k_mark_bad_k<<<64, 256, 0, cs>>>(perm, starts + nb, counts + nb, offsets, out);
   note(cudaGetLastError());
@@ -651,9 +660,18 @@ size_t api_binned_scratch(long long nsets, int form, bool all) {
   size_t qoff[kNumBins];
   return align256(sizeof(int) * (48 + (size_t)nsets)) + binned_qscratch(form, all, qoff);
 }
+int api_prepare_binned(int form, bool all) {
+  LaunchFn fns[kNumBins];
+  binned_fns(form, all, fns);
+  SetOutputs out{};
+  for (int b = 0; b < kNumBins; ++b) PL_CU(fns[b](MatrixF32{}, SetSource{}, out, 0, nullptr, 0, true));
+  return PL_OK;
+}
+
 int api_launch_binned(const MatrixF32& M, const int* idx, const long long* offsets, long long nsets,
                       int form, const SetOutputs& out, void* scratch, cudaStream_t st,
-                      const cudaStream_t* side, cudaEvent_t fork, const cudaEvent_t* join) {
+                      const cudaStream_t* side, cudaEvent_t fork, const cudaEvent_t* join,
+                      const long long* nsets_dev) {
   const bool all = out.eig || out.det;
   size_t qoff[kNumBins];
   binned_qscratch(form, all, qoff);
@@ -662,7 +680,7 @@ int api_launch_binned(const MatrixF32& M, const int* idx, const long long* offse
   char* base = (char*)scratch;
   int* hdr = (int*)base;
   char* q = base + align256(sizeof(int) * (48 + (size_t)nsets));
-  PL_CU(enqueue_binned(M, idx, offsets, nsets, out, fns, hdr, q, qoff, st, side, fork, join));
+  PL_CU(enqueue_binned(M, idx, offsets, nsets, out, fns, hdr, q, qoff, st, side, fork, join, nsets_dev));
   return PL_OK;
 }
 void api_note_cuda(cudaError_t e) { g_last_cuda = (int)e; }
@@ -998,6 +1016,33 @@ int pl_fp32_peak(double* tflops, void* stream) {
   const double flops = 2.0 * 8 * 16 * (double)iters * grid * 256;
   *tflops = flops / (ms * 1e-3) / 1e12;
   PL_CU(cudaGetLastError());
+  return PL_OK;
+}
+
+int pl_gather_peak(double* gelems, void* stream) {
+  if (!gelems) return PL_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  float* buf = nullptr;
+  PL_CU(cudaMalloc(&buf, sizeof(float) * ((size_t)1 << 24) + 256));
+  cudaError_t e = cudaMemsetAsync(buf, 0, sizeof(float) * ((size_t)1 << 24) + 256, st);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  const int grid = device_sms() * 4, iters = 200;
+  float ms = 0.f;
+  if (e == cudaSuccess) {
+    k_gather_peak<<<grid, 256, 0, st>>>(buf, 20, buf + ((size_t)1 << 24));  // warm-up: A into L2
+    cudaEventRecord(e0, st);
+    k_gather_peak<<<grid, 256, 0, st>>>(buf, iters, buf + ((size_t)1 << 24));
+    cudaEventRecord(e1, st);
+    e = cudaEventSynchronize(e1);
+  }
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(buf);
+  PL_CU(e);
+  *gelems = 16.0 * iters * (double)grid * 256 / (ms * 1e-3) / 1e9;
   return PL_OK;
 }
 

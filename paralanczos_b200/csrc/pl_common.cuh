@@ -65,8 +65,10 @@ struct SetMatrix {
   long long lda;
   int n;
   bool local;  // indices are block-local 0..k-1 (pre-formed block)
+  // A set's indices are read once per solve: a streaming (evict-first) load,
+  // so the index stream does not push the rows of A out of L2.
   __device__ __forceinline__ int index(const int* __restrict__ S, int c) const {
-    return local ? c : __ldg(S + c);
+    return local ? c : __ldcs(S + c);
   }
 };
 

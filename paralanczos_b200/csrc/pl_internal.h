@@ -23,10 +23,17 @@ size_t api_binned_scratch(long long nsets, int form, bool all);
 // counting sort of the sets by k bin, then one persistent kernel per bin on
 // the side streams side[0..nbins) (fork/join through the given events).
 // `scratch` holds api_binned_scratch(nsets, ...) bytes used by this launch
-// alone until it completes.
+// alone until it completes.  With nsets_dev non-null the set count is read
+// on the device when the launch runs (nsets is then its upper bound), so the
+// same enqueued work can be captured once and replayed for changing counts.
 int api_launch_binned(const MatrixF32& M, const int* idx, const long long* offsets, long long nsets,
                       int form, const SetOutputs& out, void* scratch, cudaStream_t st,
-                      const cudaStream_t* side, cudaEvent_t fork, const cudaEvent_t* join);
+                      const cudaStream_t* side, cudaEvent_t fork, const cudaEvent_t* join,
+                      const long long* nsets_dev = nullptr);
+
+// Loads the binned launch's kernels of `form` and caches their launch
+// attributes, so that api_launch_binned can then run inside a stream capture.
+int api_prepare_binned(int form, bool all);
 
 // Serialises calls that touch the per-device cached state.
 std::mutex& api_mutex();

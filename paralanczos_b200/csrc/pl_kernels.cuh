@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(256, 1)
 // Large-k batched form on thread-block clusters (pl_cluster.cuh): persistent,
 // one set per cluster of CS CTAs at a time.
 // ---------------------------------------------------------------------------
-template <int KB, int CS, int NTC, int RPT = 1>
+template <int KB, int CS, int NTC, int RPT = 1, bool SPLIT = false>
 __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(NTC, 1)
     k_cluster_solve(MatrixF32 M, SetSource src, SetOutputs out) {
   extern __shared__ __align__(16) float dsm[];
@@ -262,7 +262,10 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(NTC, 1)
       if (rank == 0 && threadIdx.x == 0) write_failed(out, set, off, 0, SET_BAD_K);
       continue;
     }
-    cluster_solve_set<KB, CS, NTC, RPT>(M, src.idx + off, k, set, out, sm, cl, rank);
+    if constexpr (CS == 1 || !SPLIT)
+      cluster_solve_set<KB, CS, NTC, RPT>(M, src.idx + off, k, set, out, sm, cl, rank);
+    else
+      cluster_solve_set_split<KB, CS, NTC, RPT>(M, src.idx + off, k, set, out, sm, cl, rank);
   }
 }
 
@@ -282,9 +285,12 @@ __device__ __forceinline__ int bin_of(const BinTable& bt, int k) {
   return bt.nb;  // overflow bin (k too large): reported per set
 }
 
-// counts[0..nb] (nb+1 entries, last = overflow) must be zero on entry.
+// counts[0..nb] (nb+1 entries, last = overflow) must be zero on entry.  A
+// non-null nsets_dev holds the set count on the device (nsets is then its
+// upper bound, used for the launch shape only).
 __global__ void k_bin_count(const long long* __restrict__ offsets, long long nsets, BinTable bt,
-                            int* __restrict__ counts) {
+                            int* __restrict__ counts, const long long* __restrict__ nsets_dev) {
+  if (nsets_dev) nsets = *nsets_dev;
   __shared__ int h[kMaxBins + 1];
   if (threadIdx.x <= kMaxBins) h[threadIdx.x] = 0;
   __syncthreads();
@@ -312,7 +318,8 @@ __global__ void k_bin_scan(const int* __restrict__ counts, int nb, int* __restri
 
 __global__ void k_bin_scatter(const long long* __restrict__ offsets, long long nsets, BinTable bt,
                               const int* __restrict__ starts, int* __restrict__ cursor,
-                              int* __restrict__ perm) {
+                              int* __restrict__ perm, const long long* __restrict__ nsets_dev) {
+  if (nsets_dev) nsets = *nsets_dev;
   for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nsets;
        s += (long long)gridDim.x * blockDim.x) {
     const int k = (int)(offsets[s + 1] - offsets[s]);
@@ -353,7 +360,9 @@ __global__ void k_f64_to_f32(const double* __restrict__ in, float* __restrict__ 
 // straight from registers and as tile (J, I) through a shared-memory
 // transpose.  Warp w of the 8 owns tile rows w, w + 8, ...; lane l columns
 // l and l + 32; every load of a tile is issued before the first is used, and
-// every global write is a coalesced 128-byte row segment.  err[s] =
+// every global write is a coalesced 128-byte row segment.  The blocks are
+// written and the indices read with streaming (evict-first) accesses, so that
+// they do not push A out of L2, where its random elements are found.  err[s] =
 // SET_BAD_INDEX for an index outside [0, n) (its block is left as zeros).
 constexpr int kGTile = 64, kGRows = kGTile / 8;
 
@@ -396,7 +405,7 @@ __device__ __forceinline__ void gather_tile(const float* __restrict__ A, long lo
       for (int h = 0; h < 2; ++h) {
         const int c = lane + 32 * h;
         T[c][r] = e[u][h];
-        if (r0 + r < k && c0 + c < k) out[(size_t)(r0 + r) * k + c0 + c] = e[u][h];
+        if (r0 + r < k && c0 + c < k) __stcs(out + (size_t)(r0 + r) * k + c0 + c, e[u][h]);
       }
     }
   }
@@ -408,13 +417,13 @@ __device__ __forceinline__ void gather_tile(const float* __restrict__ A, long lo
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int c = lane + 32 * h;
-      if (c0 + r < k && r0 + c < k) out[(size_t)(c0 + r) * k + r0 + c] = T[r][c];
+      if (c0 + r < k && r0 + c < k) __stcs(out + (size_t)(c0 + r) * k + r0 + c, T[r][c]);
     }
   }
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(256) k_gather_blocks(const float* __restrict__ A, int n, long long lda,
+__global__ void __launch_bounds__(256, 4) k_gather_blocks(const float* __restrict__ A, int n, long long lda,
                                                       const int* __restrict__ idx, long long nsets, int k,
                                                       float* __restrict__ blocks, int* __restrict__ err) {
   __shared__ int sidx[512];
@@ -424,14 +433,14 @@ __global__ void __launch_bounds__(256) k_gather_blocks(const float* __restrict__
   for (long long s = blockIdx.x; s < nsets; s += gridDim.x) {
     int bad = 0;
     for (int c = threadIdx.x; c < k; c += blockDim.x) {
-      const int v = __ldg(idx + s * k + c);
+      const int v = __ldcs(idx + s * k + c);
       bad |= (v < 0) | (v >= n);
       sidx[c] = v;
     }
     bad = __syncthreads_or(bad);
     float* __restrict__ out = blocks + s * kk;
     if (bad) {
-      for (long long e = threadIdx.x; e < kk; e += blockDim.x) out[e] = 0.f;
+      for (long long e = threadIdx.x; e < kk; e += blockDim.x) __stcs(out + e, 0.f);
     } else {
       for (int I = 0; I < nt; ++I)
         for (int J = I; J < nt; ++J) gather_tile(A, lda, sidx, k, I, J, out, T);
@@ -447,6 +456,35 @@ __global__ void k_gen_sets(unsigned long long seed, long long first, long long n
   for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nsets;
        s += (long long)gridDim.x * blockDim.x)
     gen_set(seed, (unsigned long long)(first + s), n, k, idx + s * (long long)k);
+}
+
+// Random-gather throughput probe: every thread issues 16 independent 4-byte
+// loads per iteration from uniformly random positions of an (L2-resident)
+// array of 2^24 floats -- the access pattern of the A[S,S] gather, where each
+// element is its own L1 request and 32-byte sector.
+__device__ __forceinline__ unsigned mix32(unsigned x) {
+  x ^= x >> 16;
+  x *= 0x7feb352dU;
+  x ^= x >> 15;
+  x *= 0x846ca68bU;
+  x ^= x >> 16;
+  return x;
+}
+
+__global__ void __launch_bounds__(256) k_gather_peak(const float* __restrict__ a, int iters, float* out) {
+  float acc = 0.f;
+  unsigned h = mix32(blockIdx.x * blockDim.x + threadIdx.x + 1u);
+  for (int it = 0; it < iters; ++it) {
+    float e[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      h = mix32(h + (unsigned)u);
+      e[u] = __ldg(a + (h & ((1u << 24) - 1u)));
+    }
+#pragma unroll
+    for (int u = 0; u < 16; ++u) acc += e[u];
+  }
+  if (acc == 1.2345f) out[0] = acc;  // keeps the loads live
 }
 
 // FP32 FMA throughput probe (8 independent chains per thread).

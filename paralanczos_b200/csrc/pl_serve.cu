@@ -1,44 +1,51 @@
-// pl_serve.cu -- serving: continuous batching of subset-eigensolve requests.
+// pl_serve.cu -- serving: continuous batching in a device-resident request loop.
 //
 // The reference has no serving layer: each calculate_subeigs* call
 // (ParaLanczos.cu:1725-1863) uploads one matrix and one batch of sets,
 // launches, copies back and resets the device.  Here a server keeps several
 // matrices resident and solves requests -- (matrix, k, a batch of index sets)
-// -- as they arrive:
+// -- as they arrive, with the batching done on the GPU:
 //
-//   * submit() copies the request's indices into a pinned host pool and
-//     queues it (PL_EBUSY when the pool is full: back-pressure);
-//   * a scheduler thread admits queued requests in arrival order while their
-//     indices fit the HBM budget arena (uploaded at admission, resident until
-//     the request completes);
-//   * work runs in "waves": a CSR batch of pieces (consecutive sets of one
-//     request) whose sets may name different matrices and k, binned by k on
-//     the device and solved by the persistent per-bin kernels of the batched
-//     form on the wave's own streams.  A wave is sized to about
-//     PL_SERVE_WAVE_MS (default 20) ms of estimated GPU work: the oldest
-//     unfinished request gets up to PL_SERVE_OLDEST_SHARE (default 0.9) of
-//     it, then requests with the
-//     least remaining work fill the rest, so a large request is split over
-//     waves while small requests that arrive behind it go out in the next
-//     wave instead of waiting for it to finish;
-//   * up to `max_waves` waves are in flight at once, each with its own stream
-//     set, staging and kernel scratch, so requests that arrive while others
-//     run are admitted as memory and wave slots free up and their kernels
-//     overlap on the GPU;
-//   * a finished wave's results are copied to pinned host memory; a request
-//     completes with its last piece (host timestamps give the latency from
-//     submit to completion) and its arena block is freed.
+//   * submit() copies the request's indices into a pinned (device-mapped)
+//     host pool and queues it (PL_EBUSY when the pool is full: back-pressure);
+//   * the host admits queued requests in arrival order while their indices
+//     fit the device arena, uploads them, and then publishes one descriptor
+//     per request into a descriptor ring in mapped host memory;
+//   * a request loop runs on the device: one CUDA graph per loop whose body
+//     sits under a conditional WHILE node -- a planning kernel, an expansion
+//     kernel, the binned launch of the batched form (device counting sort by
+//     k, one persistent kernel per k bin), and a completion kernel -- and
+//     repeats without the host.  Each pass the planning kernel absorbs new
+//     descriptors into the loop's table of active requests and forms the next
+//     "wave" of about PL_SERVE_WAVE_MS (default 20) ms of estimated GPU work:
+//     the oldest unfinished request gets up to PL_SERVE_OLDEST_SHARE (default
+//     0.9) of it, then the requests with the least work left fill the rest, so
+//     large requests are split over waves and small ones that arrive behind
+//     them go out in the next wave.  The expansion kernel lays the wave's sets
+//     out as one CSR batch (indices copied from the arena, per-set matrix ids);
+//     the completion kernel writes each set's results straight into its
+//     request's mapped host buffers and, with the last set of a request, its
+//     completion flag;
+//   * when a loop has nothing to do, its planning kernel polls the ring
+//     (bounded by %globaltimer, PL_SERVE_IDLE_MS, default 20 ms) and then ends
+//     the loop (the graph finishes, status "idle"); the host launches it again
+//     when the next descriptor is published.  Every device wait is bounded;
+//   * requests are spread over up to four loops by k (small k apart from large
+//     k), so small requests never wait behind a long large-k wave, and the
+//     loops' kernels overlap on the GPU;
+//   * all device memory of the server -- arena, wave staging, kernel scratch,
+//     tables -- is allocated at creation inside budget_bytes.
 // A set's result does not depend on what else is in its wave: each set is
-// solved by the bin's kernel on its own data with a fixed reduction order.
+// solved by its bin's kernel on its own data with a fixed reduction order.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
-#include <cmath>
 #include <atomic>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <deque>
 #include <map>
@@ -50,12 +57,19 @@
 #include "../../include/paralanczos.h"
 #include "pl_common.cuh"
 #include "pl_internal.h"
+#include "pl_sync.cuh"
 
 namespace pl {
 namespace serve {
 
 constexpr int kMaxMatrices = 64;
 constexpr int kMaxBinsS = 16;
+constexpr int kMaxLoops = 4;
+constexpr int kSlots = 1024;            // requests active on one loop at once
+constexpr int kRing = 4096;             // descriptor ring entries per loop
+constexpr long long kWaveSets = 1 << 16;  // sets one wave can hold
+constexpr long long kWaveIdx = 1 << 22;   // indices one wave can hold (16 MiB)
+constexpr int kMaxPieces = 2048;        // request pieces one wave can hold
 
 double now_s() {
   using namespace std::chrono;
@@ -108,14 +122,231 @@ struct Arena {
       }
     }
   }
-  size_t largest() const {
-    size_t m = 0;
-    for (auto& kv : free_) m = std::max(m, kv.second);
-    return m;
-  }
 };
 
-enum ReqState { PENDING = 0, ADMITTED = 1, DONE = 2, FAILED = 3 };
+// Whole-GPU time of one set of size k (microseconds), from the batched
+// kernels' B200 throughput at each bin's largest k, scaled by (k / kmax)^3
+// inside a bin and never below the previous bin's figure.  Only used to size
+// waves: a misestimate changes wave lengths, never results.
+__host__ __device__ inline double set_cost_us(int k) {
+  const int kb[9] = {8, 16, 32, 64, 128, 192, 256, 384, 512};
+  const double tb[9] = {0.001, 0.003, 0.014, 0.10, 0.88, 8.3, 25.5, 92.0, 253.0};
+  for (int b = 0; b < 9; ++b) {
+    if (k <= kb[b]) {
+      const double x = (double)k / kb[b];
+      const double c = tb[b] * x * x * x;
+      const double lo = b ? tb[b - 1] : 0.0;
+      return c > lo ? c : lo;
+    }
+  }
+  return tb[8];
+}
+
+// ---- shared host / device structures -----------------------------------------
+// One admitted request, published by the host into a loop's ring (mapped
+// pinned memory): its indices are already in the device arena.
+struct RingDesc {
+  long long id, nsets, arena_off;  // arena_off: first index, in ints
+  double *lmin, *lmax, *delta;     // device views of the request's pinned results
+  int* err;
+  int slot, mat, k, pad;
+};
+
+// A loop's control block (mapped pinned memory).
+struct Ctl {
+  long long tail;              // host: descriptors published
+  long long head;              // device: descriptors absorbed
+  long long waves;             // device: waves formed
+  int stop;                    // host: 1 = leave the loop
+  int status;                  // device: 1 running, 2 left idle, 3 left on stop
+  long long done_id[kSlots];   // device: id of the request completed in a slot
+};
+
+// Device-side state of an active request.
+struct DevReq {
+  long long id, nsets, next, done, arena_off;
+  double *lmin, *lmax, *delta;
+  int* err;
+  int mat, k;
+};
+
+struct Piece {
+  long long first, count;  // sets [first, first + count) of the request
+  long long set0, idx0;    // its first set and first index in the wave
+  int slot, k;
+};
+
+// A loop's planning state (device memory).
+struct Plan {
+  long long head;   // ring entries absorbed
+  long long nsets;  // sets of the current wave (read by the binned launch)
+  int nact, npieces;
+  int act[kSlots];  // slots with unfinished sets, in arrival order
+  Piece pieces[kMaxPieces];
+};
+
+struct LoopArgs {
+  Ctl* ctl;
+  const RingDesc* ring;
+  DevReq* tab;
+  Plan* plan;
+  const int* arena;
+  int* widx;
+  long long* woff;
+  int* wmat;
+  int* wslot;
+  long long* wpos;
+  double* wres;  // lmin, lmax, delta: kWaveSets each
+  int* werr;
+  cudaGraphConditionalHandle cond;
+  unsigned long long idle_ns;
+  double wave_us, oldest_share;
+};
+
+__device__ __forceinline__ long long ld_acquire_sys(const long long* p) {
+  long long v;
+  asm volatile("ld.acquire.sys.global.s64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release_sys(long long* p, long long v) {
+  asm volatile("st.release.sys.global.s64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Planning (one thread): retire finished requests, absorb new descriptors,
+// wait for work at most idle_ns, form the next wave or end the loop.
+__global__ void k_loop_plan(LoopArgs a) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  Plan& P = *a.plan;
+  int n = 0;
+  for (int i = 0; i < P.nact; ++i) {
+    const int s = P.act[i];
+    if (a.tab[s].done < a.tab[s].nsets) P.act[n++] = s;
+  }
+  P.nact = n;
+  const unsigned long long t0 = globaltimer();
+  for (;;) {
+    const long long tail = ld_acquire_sys(&a.ctl->tail);
+    while (P.head < tail && P.nact < kSlots) {
+      const RingDesc d = a.ring[P.head % kRing];
+      a.tab[d.slot] = DevReq{d.id, d.nsets, 0, 0, d.arena_off, d.lmin, d.lmax, d.delta, d.err, d.mat, d.k};
+      P.act[P.nact++] = d.slot;
+      ++P.head;
+    }
+    *(volatile long long*)&a.ctl->head = P.head;
+    const int stop = *(volatile int*)&a.ctl->stop;
+    bool work = false;
+    for (int i = 0; i < P.nact && !work; ++i) work = a.tab[P.act[i]].next < a.tab[P.act[i]].nsets;
+    if (work && !stop) break;
+    if (stop || globaltimer() - t0 > a.idle_ns) {
+      P.nsets = 0;
+      P.npieces = 0;
+      *(volatile int*)&a.ctl->status = stop ? 3 : 2;
+      cudaGraphSetConditional(a.cond, 0);
+      return;
+    }
+    __nanosleep(2000);
+  }
+  // the wave: the oldest unfinished request first (up to oldest_share of it),
+  // then the requests with the least work left
+  double used = 0.0;
+  long long ns = 0, ni = 0;
+  int np = 0;
+  auto take = [&](int slot, double allow) {
+    DevReq& r = a.tab[slot];
+    const long long avail = r.nsets - r.next;
+    long long room = kWaveSets - ns;
+    const long long iroom = (kWaveIdx - ni) / r.k;
+    room = room < iroom ? room : iroom;
+    if (avail <= 0 || room <= 0 || np >= kMaxPieces) return;
+    const double c = set_cost_us(r.k);
+    long long m = (long long)floor(allow / c);
+    m = m < avail ? m : avail;
+    m = m < room ? m : room;
+    m = m > 1 ? m : 1;
+    P.pieces[np++] = Piece{r.next, m, ns, ni, slot, r.k};
+    r.next += m;
+    ns += m;
+    ni += m * r.k;
+    used += m * c;
+  };
+  for (int i = 0; i < P.nact; ++i)
+    if (a.tab[P.act[i]].next < a.tab[P.act[i]].nsets) {
+      take(P.act[i], a.oldest_share * a.wave_us);
+      break;
+    }
+  while (used < a.wave_us && ns < kWaveSets && ni < kWaveIdx && np < kMaxPieces) {
+    int best = -1;
+    double bw = 0.0;
+    for (int i = 0; i < P.nact; ++i) {
+      const DevReq& r = a.tab[P.act[i]];
+      if (r.next >= r.nsets) continue;
+      const double w = (double)(r.nsets - r.next) * set_cost_us(r.k);
+      if (best < 0 || w < bw) {
+        best = P.act[i];
+        bw = w;
+      }
+    }
+    if (best < 0) break;
+    take(best, a.wave_us - used);
+  }
+  P.npieces = np;
+  P.nsets = ns;
+  *(volatile long long*)&a.ctl->waves = *(volatile long long*)&a.ctl->waves + 1;
+  cudaGraphSetConditional(a.cond, 1);
+}
+
+// The wave as one CSR batch: a warp per set copies its indices from the arena.
+__global__ void __launch_bounds__(256) k_loop_expand(LoopArgs a) {
+  const Plan& P = *a.plan;
+  const long long ns = P.nsets;
+  const int lane = threadIdx.x & 31;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long s = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < ns; s += nw) {
+    int lo = 0, hi = P.npieces - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (P.pieces[mid].set0 <= s) lo = mid; else hi = mid - 1;
+    }
+    const Piece pc = P.pieces[lo];
+    const long long j = s - pc.set0, pos = pc.first + j, off = pc.idx0 + j * pc.k;
+    const DevReq& r = a.tab[pc.slot];
+    const int* __restrict__ src = a.arena + r.arena_off + pos * pc.k;
+    for (int i = lane; i < pc.k; i += 32) a.widx[off + i] = src[i];
+    if (lane == 0) {
+      a.woff[s] = off;
+      a.wmat[s] = r.mat;
+      a.wslot[s] = pc.slot;
+      a.wpos[s] = pos;
+      if (s == ns - 1) a.woff[ns] = off + pc.k;
+    }
+  }
+}
+
+// Results into the requests' mapped host buffers; the last set of a request
+// publishes its completion flag after every result of it is visible.
+__global__ void __launch_bounds__(256) k_loop_finish(LoopArgs a) {
+  const long long ns = a.plan->nsets;
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < ns;
+       s += (long long)gridDim.x * blockDim.x) {
+    const int slot = a.wslot[s];
+    const long long pos = a.wpos[s];
+    DevReq& r = a.tab[slot];
+    r.lmin[pos] = a.wres[s];
+    r.lmax[pos] = a.wres[kWaveSets + s];
+    r.delta[pos] = a.wres[2 * kWaveSets + s];
+    r.err[pos] = a.werr[s];
+    __threadfence_system();
+    const unsigned long long prev = atomicAdd(reinterpret_cast<unsigned long long*>(&r.done), 1ull);
+    if ((long long)prev + 1 == r.nsets) {
+      __threadfence_system();
+      st_release_sys(&a.ctl->done_id[slot], r.id);
+    }
+  }
+}
+
+// ---- host side ------------------------------------------------------------------
+enum ReqState { PENDING = 0, UPLOADING = 1, PUBLISHED = 2, DONE = 3, FAILED = 4 };
 
 struct Request {
   long long id = 0;
@@ -129,92 +360,60 @@ struct Request {
   int state = PENDING;
   int status = PL_OK;
   size_t dev_off = 0, dev_len = 0;  // arena block holding the indices on the device
-  long long next = 0;               // first set not yet given to a wave
-  long long done = 0;               // sets whose results are back
+  int loop = 0, slot = -1;
 };
 
-// Arena charge of one request: its indices, resident on the device from
-// admission to completion.
 size_t req_dev_bytes(long long nsets, int k) { return a256(sizeof(int) * (size_t)nsets * k); }
 size_t req_host_bytes(long long nsets, int k) {
   return a256(sizeof(int) * (size_t)nsets * k) + a256(3 * sizeof(double) * (size_t)nsets) +
          a256(sizeof(int) * (size_t)nsets);
 }
 
-// Whole-GPU time of one set of size k (microseconds), from the batched
-// kernels' B200 throughput at each bin's largest k, scaled by (k / kmax)^3
-// inside a bin and never below the previous bin's figure.  Only used to size
-// waves: a misestimate changes wave lengths, never results.
-double set_cost_us(int k) {
-  static const int kb[9] = {8, 16, 32, 64, 128, 192, 256, 384, 512};
-  static const double tb[9] = {0.001, 0.003, 0.014, 0.10, 0.88, 8.3, 25.5, 92.0, 253.0};
-  for (int b = 0; b < 9; ++b) {
-    if (k <= kb[b]) {
-      const double x = (double)k / kb[b];
-      return std::max(tb[b] * x * x * x, b ? tb[b - 1] : 0.0);
-    }
-  }
-  return tb[8];
-}
-
-constexpr long long kWaveSets = 1 << 16;  // sets one wave can hold
-constexpr long long kWaveIdx = 1 << 24;   // indices one wave can hold (64 MiB)
-
-struct Piece {
-  Request* r;
-  long long first, count;  // sets [first, first + count) of the request
-};
-
-struct Wave {
-  cudaStream_t st = nullptr;
-  cudaStream_t side[kMaxBinsS] = {};
-  cudaEvent_t fork = nullptr, join[kMaxBinsS] = {}, done = nullptr;
+struct Loop {
+  Ctl* ctl = nullptr;  // mapped: host and device view are the same address (UVA)
+  RingDesc* ring = nullptr;
+  DevReq* tab = nullptr;
+  Plan* plan = nullptr;
+  char* dmem = nullptr;  // one device allocation: tab, plan, wave staging, scratch
+  LoopArgs args{};
   void* scratch = nullptr;
-  size_t scratch_bytes = 0;
-  // device staging of one wave: its pieces' indices gathered contiguously,
-  // CSR offsets, matrix ids, results
-  int* d_idx = nullptr;
-  long long nidx = 0;
-  long long* d_off = nullptr;
-  int* d_mat = nullptr;
-  double* d_res = nullptr;  // lmin, lmax, delta: kWaveSets each
-  int* d_err = nullptr;
-  // pinned staging
-  long long* h_off = nullptr;
-  int* h_mat = nullptr;
-  double* h_res = nullptr;
-  int* h_err = nullptr;
-  bool busy = false;
-  long long nsets = 0;
-  std::vector<Piece> pieces;
+  cudaStream_t st = nullptr, cap = nullptr;
+  cudaStream_t side[kMaxBinsS] = {};
+  cudaEvent_t fork = nullptr, join[kMaxBinsS] = {};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool running = false;
+  long long published = 0;
+  std::vector<int> free_slots;
+  std::vector<Request*> live;  // published, not complete
+  long long launches = 0, idle_exits = 0;
 };
 
 struct Server {
-  int dev = 0;
-  int nbins = 0;
-  Arena arena;  // device budget: indices of admitted requests
+  int dev = 0, nbins = 0, nloops = 1;
+  Arena arena;  // device budget left for request indices
   char* d_arena = nullptr;
-  Arena pool;   // pinned host staging
+  Arena pool;   // pinned host staging (device-mapped)
   char* h_pool = nullptr;
+  char* d_pool = nullptr;  // the pool's device address
   MatrixRef* d_mats = nullptr;
   std::vector<MatrixRef> mats;
-  std::vector<Wave> waves;
-  cudaStream_t up = nullptr;   // index uploads at admission
+  Loop loops[kMaxLoops];
+  size_t fixed_bytes = 0, budget = 0;
+  cudaStream_t up = nullptr;  // index uploads at admission
   cudaEvent_t up_ev = nullptr;
-  double wave_us = 20000.0;    // GPU work one wave is sized for
-  double oldest_share = 0.9;   // part of a wave the oldest unfinished request may take
+  std::vector<Request*> uploading;  // uploaded by up_ev, not yet published
+  double wave_us = 20000.0, oldest_share = 0.9, idle_ms = 20.0;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<Request*> pending;  // submitted, not admitted (arrival order)
-  std::vector<Request*> active;  // admitted, not complete (arrival order)
   std::unordered_map<long long, Request*> reqs;
   std::thread th;
   std::atomic<bool> stop{false};
   long long next_id = 1;
-  // statistics
   std::vector<double> lat;
-  long long sets_done = 0, waves_launched = 0;
-  int inflight_max = 0;
+  long long sets_done = 0;
+  int running_max = 0;
   double t_first = 0, t_last = 0;
 };
 
@@ -223,158 +422,136 @@ int cuda_fail(cudaError_t e) {
   return e == cudaErrorMemoryAllocation ? PL_ENOMEM : PL_ECUDA;
 }
 
-int wave_alloc(Wave& w) {
-  const size_t n = (size_t)kWaveSets;
+// Loop of a request: small k apart from large k (upper k of loop i).
+int loop_of(const Server& S, int k) {
+  static const int edges[kMaxLoops + 1][kMaxLoops] = {
+      {0}, {1 << 30}, {128, 1 << 30}, {64, 192, 1 << 30}, {32, 128, 256, 1 << 30}};
+  for (int i = 0; i < S.nloops; ++i)
+    if (k <= edges[S.nloops][i]) return i;
+  return S.nloops - 1;
+}
+
+// Device bytes of one loop (tables, wave staging, binned-launch scratch).
+struct LoopLayout {
+  size_t tab, plan, widx, woff, wmat, wslot, wpos, wres, werr, scratch, total;
+};
+LoopLayout loop_layout() {
+  LoopLayout L;
+  size_t o = 0;
+  auto take = [&](size_t n) {
+    const size_t at = o;
+    o += a256(n);
+    return at;
+  };
+  L.tab = take(sizeof(DevReq) * kSlots);
+  L.plan = take(sizeof(Plan));
+  L.widx = take(sizeof(int) * (size_t)kWaveIdx);
+  L.woff = take(sizeof(long long) * (size_t)(kWaveSets + 1));
+  L.wmat = take(sizeof(int) * (size_t)kWaveSets);
+  L.wslot = take(sizeof(int) * (size_t)kWaveSets);
+  L.wpos = take(sizeof(long long) * (size_t)kWaveSets);
+  L.wres = take(3 * sizeof(double) * (size_t)kWaveSets);
+  L.werr = take(sizeof(int) * (size_t)kWaveSets);
+  L.scratch = take(api_binned_scratch(kWaveSets, PL_FORM_BATCHED, false));
+  L.total = o;
+  return L;
+}
+
+// The loop's graph: WHILE(cond) { plan; expand; binned solve; finish }.
+int build_loop(Server& S, Loop& L) {
+  const LoopLayout lay = loop_layout();
   cudaError_t e;
-  if ((e = cudaMalloc(&w.d_idx, sizeof(int) * (size_t)kWaveIdx)) != cudaSuccess) return cuda_fail(e);
-  if ((e = cudaMalloc(&w.d_off, sizeof(long long) * (n + 1))) != cudaSuccess) return cuda_fail(e);
-  if ((e = cudaMalloc(&w.d_mat, sizeof(int) * n)) != cudaSuccess) return cuda_fail(e);
-  if ((e = cudaMalloc(&w.d_res, 3 * sizeof(double) * n)) != cudaSuccess) return cuda_fail(e);
-  if ((e = cudaMalloc(&w.d_err, sizeof(int) * n)) != cudaSuccess) return cuda_fail(e);
-  if ((e = cudaHostAlloc(&w.h_off, sizeof(long long) * (n + 1), 0)) != cudaSuccess) return cuda_fail(e);
-  if ((e = cudaHostAlloc(&w.h_mat, sizeof(int) * n, 0)) != cudaSuccess) return cuda_fail(e);
-  if ((e = cudaHostAlloc(&w.h_res, 3 * sizeof(double) * n, 0)) != cudaSuccess) return cuda_fail(e);
-  if ((e = cudaHostAlloc(&w.h_err, sizeof(int) * n, 0)) != cudaSuccess) return cuda_fail(e);
-  return PL_OK;
-}
+  if ((e = cudaMalloc(&L.dmem, lay.total)) != cudaSuccess) return cuda_fail(e);
+  if ((e = cudaMemset(L.dmem, 0, lay.tab + lay.plan + sizeof(Plan))) != cudaSuccess) return cuda_fail(e);
+  if ((e = cudaHostAlloc(&L.ctl, sizeof(Ctl), cudaHostAllocMapped)) != cudaSuccess) return cuda_fail(e);
+  if ((e = cudaHostAlloc(&L.ring, sizeof(RingDesc) * kRing, cudaHostAllocMapped)) != cudaSuccess)
+    return cuda_fail(e);
+  memset(L.ctl, 0, sizeof(Ctl));
+  for (int i = 0; i < kSlots; ++i) L.ctl->done_id[i] = -1;
+  L.tab = (DevReq*)(L.dmem + lay.tab);
+  L.plan = (Plan*)(L.dmem + lay.plan);
+  L.scratch = L.dmem + lay.scratch;
+  for (int i = kSlots - 1; i >= 0; --i) L.free_slots.push_back(i);
+  Ctl* ctl_d = nullptr;
+  RingDesc* ring_d = nullptr;
+  if ((e = cudaHostGetDevicePointer((void**)&ctl_d, L.ctl, 0)) != cudaSuccess) return cuda_fail(e);
+  if ((e = cudaHostGetDevicePointer((void**)&ring_d, L.ring, 0)) != cudaSuccess) return cuda_fail(e);
+  LoopArgs& a = L.args;
+  a.ctl = ctl_d;
+  a.ring = ring_d;
+  a.tab = L.tab;
+  a.plan = L.plan;
+  a.arena = (const int*)S.d_arena;
+  a.widx = (int*)(L.dmem + lay.widx);
+  a.woff = (long long*)(L.dmem + lay.woff);
+  a.wmat = (int*)(L.dmem + lay.wmat);
+  a.wslot = (int*)(L.dmem + lay.wslot);
+  a.wpos = (long long*)(L.dmem + lay.wpos);
+  a.wres = (double*)(L.dmem + lay.wres);
+  a.werr = (int*)(L.dmem + lay.werr);
+  a.idle_ns = (unsigned long long)(S.idle_ms * 1e6);
+  a.wave_us = S.wave_us;
+  a.oldest_share = S.oldest_share;
+  if ((e = cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaStreamCreateWithFlags(&L.cap, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&L.fork, cudaEventDisableTiming)) != cudaSuccess)
+    return cuda_fail(e);
+  for (int b = 0; b < S.nbins; ++b)
+    if ((e = cudaStreamCreateWithFlags(&L.side[b], cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&L.join[b], cudaEventDisableTiming)) != cudaSuccess)
+      return cuda_fail(e);
 
-int wave_scratch(Wave& w, long long nsets) {
-  const size_t need = api_binned_scratch(nsets, PL_FORM_BATCHED, false);
-  if (w.scratch_bytes >= need) return PL_OK;
-  if (w.scratch) cudaFree(w.scratch);
-  w.scratch = nullptr;
-  w.scratch_bytes = 0;
-  cudaError_t e = cudaMalloc(&w.scratch, need);
-  if (e != cudaSuccess) return cuda_fail(e);
-  w.scratch_bytes = need;
-  return PL_OK;
-}
-
-// Pieces of the next wave (server lock held): the oldest unfinished request
-// first gets up to oldest_share of the wave (no request waits forever), then
-// requests in order of least remaining work fill the rest, so a small
-// request arriving behind a large one finishes in the next wave while the
-// large one advances a wave at a time.  Every piece has at least one set.
-void form_wave(Server& S, Wave& w) {
-  w.pieces.clear();
-  w.nsets = 0;
-  w.nidx = 0;
-  double used = 0.0;
-  auto take = [&](Request* r, double allow) {
-    const long long avail = r->nsets - r->next;
-    const long long room = std::min(kWaveSets - w.nsets, (kWaveIdx - w.nidx) / r->k);
-    if (avail <= 0 || room <= 0) return;
-    const double c = set_cost_us(r->k);
-    long long n = (long long)std::floor(allow / c);
-    n = std::max(1LL, std::min(n, std::min(avail, room)));
-    if (!w.pieces.empty() && w.pieces.back().r == r && w.pieces.back().first + w.pieces.back().count == r->next)
-      w.pieces.back().count += n;
-    else
-      w.pieces.push_back(Piece{r, r->next, n});
-    r->next += n;
-    w.nsets += n;
-    w.nidx += n * r->k;
-    used += n * c;
-  };
-  Request* oldest = nullptr;
-  for (Request* r : S.active)
-    if (r->next < r->nsets) {
-      oldest = r;
-      break;
-    }
-  if (!oldest) return;
-  take(oldest, S.oldest_share * S.wave_us);
-  std::vector<Request*> order;
-  for (Request* r : S.active)
-    if (r->next < r->nsets) order.push_back(r);
-  std::stable_sort(order.begin(), order.end(), [](const Request* a, const Request* b) {
-    return (a->nsets - a->next) * set_cost_us(a->k) < (b->nsets - b->next) * set_cost_us(b->k);
-  });
-  for (Request* r : order) {
-    if (used >= S.wave_us || w.nsets >= kWaveSets || w.nidx >= kWaveIdx) break;
-    take(r, S.wave_us - used);
-  }
-}
-
-// Enqueue one wave (scheduler thread, server lock NOT held; m0 is any
-// registered matrix, read under the lock).
-int launch_wave(Server& S, Wave& w, MatrixRef m0) {
-  const long long total = w.nsets;
-  cudaError_t e = cudaSuccess;
-  auto note = [&](cudaError_t x) {
-    if (e == cudaSuccess && x != cudaSuccess) e = x;
-  };
-  note(cudaStreamWaitEvent(w.st, S.up_ev, 0));  // the pieces' indices are on the device
-  long long s = 0, o = 0;
-  for (const Piece& p : w.pieces) {
-    const long long cnt = p.count * p.r->k;
-    note(cudaMemcpyAsync(w.d_idx + o, S.d_arena + p.r->dev_off + sizeof(int) * (size_t)(p.first * p.r->k),
-                         sizeof(int) * (size_t)cnt, cudaMemcpyDeviceToDevice, w.st));
-    for (long long i = 0; i < p.count; ++i, ++s) {
-      w.h_off[s] = o + i * p.r->k;
-      w.h_mat[s] = p.r->mat;
-    }
-    o += cnt;
-  }
-  w.h_off[total] = o;
-  note(cudaMemcpyAsync(w.d_off, w.h_off, sizeof(long long) * (size_t)(total + 1), cudaMemcpyHostToDevice, w.st));
-  note(cudaMemcpyAsync(w.d_mat, w.h_mat, sizeof(int) * (size_t)total, cudaMemcpyHostToDevice, w.st));
-  if (e != cudaSuccess) return cuda_fail(e);
-  MatrixF32 M{m0.A, m0.lda, m0.n};
-  M.mats = S.d_mats;
-  M.mat_id = w.d_mat;
-  const size_t n = (size_t)kWaveSets;
-  SetOutputs out{w.d_res, w.d_res + n, w.d_res + 2 * n, w.d_err, nullptr, nullptr};
+  if ((e = cudaGraphCreate(&L.graph, 0)) != cudaSuccess) return cuda_fail(e);
+  if ((e = cudaGraphConditionalHandleCreate(&a.cond, L.graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess)
+    return cuda_fail(e);
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = a.cond;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  if ((e = cudaGraphAddNode(&node, L.graph, nullptr, 0, &cp)) != cudaSuccess) return cuda_fail(e);
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
   int rc;
   {
-    // kernel shapes (and so the scratch size) may be retuned between waves
     std::lock_guard<std::mutex> lk(api_mutex());
-    rc = wave_scratch(w, total);
-    if (!rc)
-      rc = api_launch_binned(M, w.d_idx, w.d_off, total, PL_FORM_BATCHED, out, w.scratch, w.st,
-                             w.side, w.fork, w.join);
+    rc = api_prepare_binned(PL_FORM_BATCHED, false);
   }
   if (rc) return rc;
-  for (int q = 0; q < 3; ++q)
-    note(cudaMemcpyAsync(w.h_res + q * n, w.d_res + q * n, sizeof(double) * (size_t)total,
-                         cudaMemcpyDeviceToHost, w.st));
-  note(cudaMemcpyAsync(w.h_err, w.d_err, sizeof(int) * (size_t)total, cudaMemcpyDeviceToHost, w.st));
-  note(cudaEventRecord(w.done, w.st));
+  const int sms = api_device_sms();
+  if ((e = cudaStreamBeginCaptureToGraph(L.cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+      cudaSuccess)
+    return cuda_fail(e);
+  k_loop_plan<<<1, 32, 0, L.cap>>>(a);
+  k_loop_expand<<<sms * 4, 256, 0, L.cap>>>(a);
+  MatrixF32 M{nullptr, 0, 0};
+  M.mats = S.d_mats;
+  M.mat_id = a.wmat;
+  SetOutputs out{a.wres, a.wres + kWaveSets, a.wres + 2 * kWaveSets, a.werr, nullptr, nullptr};
+  {
+    std::lock_guard<std::mutex> lk(api_mutex());
+    rc = api_launch_binned(M, a.widx, a.woff, kWaveSets, PL_FORM_BATCHED, out, L.scratch, L.cap, L.side, L.fork,
+                           L.join, &L.plan->nsets);
+  }
+  k_loop_finish<<<sms * 4, 256, 0, L.cap>>>(a);
+  cudaGraph_t captured = nullptr;
+  e = cudaStreamEndCapture(L.cap, &captured);
+  if (rc) return rc;
   if (e != cudaSuccess) return cuda_fail(e);
+  if ((e = cudaGraphInstantiate(&L.exec, L.graph, 0)) != cudaSuccess) return cuda_fail(e);
   return PL_OK;
 }
 
-// Results of a finished wave -> its requests (server lock held).  A request
-// completes when its last piece is back; then its arena block is freed.
-void finish_wave(Server& S, Wave& w, int status) {
+void fail_loop(Server& S, Loop& L, int status) {
   const double t = now_s();
-  const size_t n = (size_t)kWaveSets;
-  long long s = 0;
-  for (const Piece& p : w.pieces) {
-    Request* r = p.r;
-    if (status == PL_OK) {
-      const size_t bytes = sizeof(double) * (size_t)p.count;
-      memcpy(r->h_res + p.first, w.h_res + s, bytes);
-      memcpy(r->h_res + r->nsets + p.first, w.h_res + n + s, bytes);
-      memcpy(r->h_res + 2 * r->nsets + p.first, w.h_res + 2 * n + s, bytes);
-      memcpy(r->h_err + p.first, w.h_err + s, sizeof(int) * (size_t)p.count);
-    } else if (r->status == PL_OK) {
-      r->status = status;
-    }
-    s += p.count;
-    r->done += p.count;
-    if (r->done == r->nsets) {
-      r->state = r->status == PL_OK ? DONE : FAILED;
-      r->t_done = t;
-      S.lat.push_back(t - r->t_submit);
-      S.t_last = t;
-      if (r->state == DONE) S.sets_done += r->nsets;
-      S.arena.release(r->dev_off, r->dev_len);
-      S.active.erase(std::find(S.active.begin(), S.active.end(), r));
-    }
+  for (Request* r : L.live) {
+    r->state = FAILED;
+    r->status = status;
+    r->t_done = t;
+    S.arena.release(r->dev_off, r->dev_len);
+    L.free_slots.push_back(r->slot);
   }
-  w.pieces.clear();
-  w.busy = false;
+  L.live.clear();
 }
 
 void scheduler(Server* sp) {
@@ -383,77 +560,114 @@ void scheduler(Server* sp) {
   std::unique_lock<std::mutex> lk(S.mu);
   while (!S.stop.load()) {
     bool progressed = false;
-    // ---- completions
-    int inflight = 0;
-    for (Wave& w : S.waves) {
-      if (!w.busy) continue;
-      const cudaError_t q = cudaEventQuery(w.done);
-      if (q == cudaSuccess) {
-        finish_wave(S, w, PL_OK);
-        progressed = true;
-      } else if (q != cudaErrorNotReady) {
-        api_note_cuda(q);
-        finish_wave(S, w, PL_ECUDA);
-        progressed = true;
-      } else {
-        ++inflight;
+    // ---- completions: flags written by the device loops
+    const double t = now_s();
+    for (int li = 0; li < S.nloops; ++li) {
+      Loop& L = S.loops[li];
+      for (size_t i = 0; i < L.live.size();) {
+        Request* r = L.live[i];
+        if (*(volatile long long*)&L.ctl->done_id[r->slot] == r->id) {
+          r->state = DONE;
+          r->t_done = t;
+          S.lat.push_back(t - r->t_submit);
+          S.t_last = t;
+          S.sets_done += r->nsets;
+          S.arena.release(r->dev_off, r->dev_len);
+          L.free_slots.push_back(r->slot);
+          L.live[i] = L.live.back();
+          L.live.pop_back();
+          progressed = true;
+        } else {
+          ++i;
+        }
       }
     }
     if (progressed) S.cv_done.notify_all();
-    // ---- admission: arrival order, while the indices fit the arena
-    bool admitted = false;
-    while (!S.pending.empty()) {
-      Request* r = S.pending.front();
-      size_t off = 0;
-      const size_t b = req_dev_bytes(r->nsets, r->k);
-      if (!S.arena.alloc(b, &off)) break;
-      r->dev_off = off;
-      r->dev_len = b;
-      r->state = ADMITTED;
-      cudaError_t e = cudaMemcpyAsync(S.d_arena + off, r->h_idx, sizeof(int) * (size_t)r->nsets * r->k,
-                                      cudaMemcpyHostToDevice, S.up);
-      if (e != cudaSuccess) api_note_cuda(e);
-      S.pending.pop_front();
-      S.active.push_back(r);
-      admitted = true;
-    }
-    if (admitted) {
-      cudaEventRecord(S.up_ev, S.up);
-      if (S.t_first == 0) S.t_first = now_s();
+    // ---- publication of the uploaded batch
+    if (!S.uploading.empty() && cudaEventQuery(S.up_ev) == cudaSuccess) {
+      for (Request* r : S.uploading) {
+        Loop& L = S.loops[r->loop];
+        RingDesc& d = L.ring[L.published % kRing];
+        const size_t nres = (size_t)r->nsets;
+        double* res = (double*)(S.d_pool + ((char*)r->h_res - S.h_pool));
+        int* err = (int*)(S.d_pool + ((char*)r->h_err - S.h_pool));
+        d = RingDesc{r->id, r->nsets, (long long)(r->dev_off / sizeof(int)), res, res + nres, res + 2 * nres,
+                     err, r->slot, r->mat, r->k, 0};
+        std::atomic_thread_fence(std::memory_order_release);
+        ++L.published;
+        *(volatile long long*)&L.ctl->tail = L.published;
+        r->state = PUBLISHED;
+        L.live.push_back(r);
+      }
+      S.uploading.clear();
       progressed = true;
     }
-    // ---- a wave into a free slot
-    Wave* free_w = nullptr;
-    for (Wave& w : S.waves)
-      if (!w.busy) {
-        free_w = &w;
-        break;
+    // ---- admission: arrival order, while the indices fit the arena and the
+    //      request's loop has a free slot and ring room
+    if (S.uploading.empty()) {
+      while (!S.pending.empty()) {
+        Request* r = S.pending.front();
+        Loop& L = S.loops[r->loop];
+        if (L.free_slots.empty()) break;
+        if (L.published - *(volatile long long*)&L.ctl->head >= kRing) break;
+        size_t off = 0;
+        const size_t b = req_dev_bytes(r->nsets, r->k);
+        if (!S.arena.alloc(b, &off)) break;
+        r->dev_off = off;
+        r->dev_len = b;
+        r->slot = L.free_slots.back();
+        L.free_slots.pop_back();
+        r->state = UPLOADING;
+        cudaError_t e = cudaMemcpyAsync(S.d_arena + off, r->h_idx, sizeof(int) * (size_t)r->nsets * r->k,
+                                        cudaMemcpyHostToDevice, S.up);
+        if (e != cudaSuccess) api_note_cuda(e);
+        S.pending.pop_front();
+        S.uploading.push_back(r);
       }
-    if (free_w) {
-      Wave& w = *free_w;
-      form_wave(S, w);
-      if (!w.pieces.empty()) {
-        w.busy = true;
-        const MatrixRef m0 = S.mats[0];
-        lk.unlock();
-        const int rc = launch_wave(S, w, m0);
-        lk.lock();
-        ++S.waves_launched;
-        if (rc) {
-          // nothing of the wave is in flight past the failed call: drain it
-          cudaStreamSynchronize(w.st);
-          finish_wave(S, w, rc);
-          S.cv_done.notify_all();
-        } else {
-          S.inflight_max = std::max(S.inflight_max, inflight + 1);
-        }
+      if (!S.uploading.empty()) {
+        cudaEventRecord(S.up_ev, S.up);
+        if (S.t_first == 0) S.t_first = now_s();
         progressed = true;
       }
     }
+    // ---- the device loops: notice ended ones, (re)launch where work waits
+    int running = 0;
+    for (int li = 0; li < S.nloops; ++li) {
+      Loop& L = S.loops[li];
+      if (L.running) {
+        const cudaError_t q = cudaStreamQuery(L.st);
+        if (q == cudaSuccess) {
+          L.running = false;
+          if (*(volatile int*)&L.ctl->status == 2) ++L.idle_exits;
+        } else if (q != cudaErrorNotReady) {
+          api_note_cuda(q);
+          L.running = false;
+          fail_loop(S, L, PL_ECUDA);
+          S.cv_done.notify_all();
+        }
+      }
+      if (!L.running && !L.live.empty()) {
+        *(volatile int*)&L.ctl->stop = 0;
+        *(volatile int*)&L.ctl->status = 1;
+        std::atomic_thread_fence(std::memory_order_release);
+        const cudaError_t e = cudaGraphLaunch(L.exec, L.st);
+        if (e != cudaSuccess) {
+          api_note_cuda(e);
+          fail_loop(S, L, PL_ECUDA);
+          S.cv_done.notify_all();
+        } else {
+          L.running = true;
+          ++L.launches;
+          progressed = true;
+        }
+      }
+      running += L.running ? 1 : 0;
+    }
+    S.running_max = std::max(S.running_max, running);
     if (!progressed) {
-      bool any_busy = false;
-      for (Wave& w : S.waves) any_busy |= w.busy;
-      if (any_busy) {
+      bool busy = !S.uploading.empty();
+      for (int li = 0; li < S.nloops; ++li) busy |= !S.loops[li].live.empty();
+      if (busy) {
         lk.unlock();
         std::this_thread::sleep_for(std::chrono::microseconds(20));
         lk.lock();
@@ -473,25 +687,22 @@ int destroy(Server* S) {
   S->cv_work.notify_all();
   if (S->th.joinable()) S->th.join();
   cudaSetDevice(S->dev);
-  for (Wave& w : S->waves) {
-    if (w.st) cudaStreamSynchronize(w.st);
-    for (int b = 0; b < S->nbins; ++b) {
-      if (w.side[b]) cudaStreamDestroy(w.side[b]);
-      if (w.join[b]) cudaEventDestroy(w.join[b]);
+  for (int li = 0; li < kMaxLoops; ++li) {
+    Loop& L = S->loops[li];
+    if (L.ctl) *(volatile int*)&L.ctl->stop = 1;  // a running loop leaves at its next poll
+    if (L.st) cudaStreamSynchronize(L.st);
+    if (L.exec) cudaGraphExecDestroy(L.exec);
+    if (L.graph) cudaGraphDestroy(L.graph);
+    for (int b = 0; b < kMaxBinsS; ++b) {
+      if (L.side[b]) cudaStreamDestroy(L.side[b]);
+      if (L.join[b]) cudaEventDestroy(L.join[b]);
     }
-    if (w.st) cudaStreamDestroy(w.st);
-    if (w.fork) cudaEventDestroy(w.fork);
-    if (w.done) cudaEventDestroy(w.done);
-    if (w.scratch) cudaFree(w.scratch);
-    cudaFree(w.d_idx);
-    cudaFree(w.d_off);
-    cudaFree(w.d_mat);
-    cudaFree(w.d_res);
-    cudaFree(w.d_err);
-    cudaFreeHost(w.h_off);
-    cudaFreeHost(w.h_mat);
-    cudaFreeHost(w.h_res);
-    cudaFreeHost(w.h_err);
+    if (L.st) cudaStreamDestroy(L.st);
+    if (L.cap) cudaStreamDestroy(L.cap);
+    if (L.fork) cudaEventDestroy(L.fork);
+    if (L.dmem) cudaFree(L.dmem);
+    if (L.ctl) cudaFreeHost(L.ctl);
+    if (L.ring) cudaFreeHost(L.ring);
   }
   if (S->up) cudaStreamSynchronize(S->up);
   if (S->up) cudaStreamDestroy(S->up);
@@ -516,52 +727,44 @@ int pl_serve_create(long long budget_bytes, long long host_pool_bytes, int max_w
   if (!server || budget_bytes < 4096 || host_pool_bytes < 4096 || max_waves < 1 || max_waves > 8)
     return PL_EINVAL;
   *server = nullptr;
+  const int nloops = std::min(max_waves, kMaxLoops);
+  const size_t fixed = nloops * loop_layout().total + a256(sizeof(MatrixRef) * kMaxMatrices);
+  if ((size_t)budget_bytes < fixed + (1u << 20)) return PL_EINVAL;  // no room for any indices
   Server* S = new Server();
   cudaGetDevice(&S->dev);
   S->nbins = api_num_bins();
+  S->nloops = nloops;
+  S->budget = (size_t)budget_bytes;
+  S->fixed_bytes = fixed;
   if (S->nbins > kMaxBinsS) {
     delete S;
     return PL_ENOTSUP;
   }
-  cudaError_t e;
-  if ((e = cudaMalloc(&S->d_arena, (size_t)budget_bytes)) != cudaSuccess ||
-      (e = cudaMalloc(&S->d_mats, sizeof(MatrixRef) * kMaxMatrices)) != cudaSuccess ||
-      (e = cudaHostAlloc(&S->h_pool, (size_t)host_pool_bytes, 0)) != cudaSuccess) {
-    destroy(S);
-    return cuda_fail(e);
-  }
-  S->arena.init((size_t)budget_bytes);
-  S->pool.init((size_t)host_pool_bytes);
   if (const char* wm = getenv("PL_SERVE_WAVE_MS")) S->wave_us = std::max(0.1, atof(wm)) * 1000.0;
   if (const char* os = getenv("PL_SERVE_OLDEST_SHARE"))
     S->oldest_share = std::min(1.0, std::max(0.05, atof(os)));
+  if (const char* im = getenv("PL_SERVE_IDLE_MS")) S->idle_ms = std::min(10000.0, std::max(0.05, atof(im)));
+  const size_t arena = (size_t)budget_bytes - fixed;
+  cudaError_t e;
+  if ((e = cudaMalloc(&S->d_arena, arena)) != cudaSuccess ||
+      (e = cudaMalloc(&S->d_mats, sizeof(MatrixRef) * kMaxMatrices)) != cudaSuccess ||
+      (e = cudaHostAlloc(&S->h_pool, (size_t)host_pool_bytes, cudaHostAllocMapped)) != cudaSuccess) {
+    destroy(S);
+    return cuda_fail(e);
+  }
+  if ((e = cudaHostGetDevicePointer((void**)&S->d_pool, S->h_pool, 0)) != cudaSuccess) {
+    destroy(S);
+    return cuda_fail(e);
+  }
+  S->arena.init(arena);
+  S->pool.init((size_t)host_pool_bytes);
   if ((e = cudaStreamCreateWithFlags(&S->up, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaEventCreateWithFlags(&S->up_ev, cudaEventDisableTiming)) != cudaSuccess) {
     destroy(S);
     return cuda_fail(e);
   }
-  S->waves.resize(max_waves);
-  for (Wave& w : S->waves) {
-    if ((e = cudaStreamCreateWithFlags(&w.st, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&w.fork, cudaEventDisableTiming)) != cudaSuccess ||
-        (e = cudaEventCreateWithFlags(&w.done, cudaEventDisableTiming)) != cudaSuccess) {
-      destroy(S);
-      return cuda_fail(e);
-    }
-    for (int b = 0; b < S->nbins; ++b) {
-      if ((e = cudaStreamCreateWithFlags(&w.side[b], cudaStreamNonBlocking)) != cudaSuccess ||
-          (e = cudaEventCreateWithFlags(&w.join[b], cudaEventDisableTiming)) != cudaSuccess) {
-        destroy(S);
-        return cuda_fail(e);
-      }
-    }
-    // staging and kernel scratch of a full wave up front: growing them later
-    // frees memory, which waits for the device
-    int rc = wave_alloc(w);
-    if (!rc) {
-      std::lock_guard<std::mutex> lk(api_mutex());
-      rc = wave_scratch(w, kWaveSets);
-    }
+  for (int li = 0; li < nloops; ++li) {
+    const int rc = build_loop(*S, S->loops[li]);
     if (rc) {
       destroy(S);
       return rc;
@@ -604,6 +807,7 @@ int pl_serve_submit(void* server, int matrix_id, const int* idx, long long nsets
   r->mat = matrix_id;
   r->k = k;
   r->nsets = nsets;
+  r->loop = loop_of(*S, k);
   r->host_off = hoff;
   r->host_len = hb;
   char* hp = S->h_pool + hoff;
@@ -665,7 +869,16 @@ int pl_serve_stats(void* server, double* out, int nout) {
   double mean = 0;
   for (double x : l) mean += x;
   if (!l.empty()) mean /= (double)l.size();
-  const double v[12] = {(double)l.size(),
+  long long waves = 0, launches = 0, idle = 0;
+  int running = 0;
+  for (int li = 0; li < S->nloops; ++li) {
+    const Loop& L = S->loops[li];
+    waves += *(volatile long long*)&L.ctl->waves;
+    launches += L.launches;
+    idle += L.idle_exits;
+    running += L.running ? 1 : 0;
+  }
+  const double v[16] = {(double)l.size(),
                         (double)S->sets_done,
                         pct(0.50),
                         pct(0.99),
@@ -674,10 +887,14 @@ int pl_serve_stats(void* server, double* out, int nout) {
                         S->t_last > S->t_first ? S->t_last - S->t_first : 0.0,
                         (double)S->arena.peak,
                         (double)S->arena.size,
-                        (double)S->waves_launched,
-                        (double)S->inflight_max,
-                        (double)S->pending.size()};
-  for (int i = 0; i < nout && i < 12; ++i) out[i] = v[i];
+                        (double)waves,
+                        (double)S->running_max,
+                        (double)S->pending.size(),
+                        (double)launches,
+                        (double)idle,
+                        (double)(S->fixed_bytes + S->arena.size),
+                        (double)running};
+  for (int i = 0; i < nout && i < 16; ++i) out[i] = v[i];
   return PL_OK;
 }
 
@@ -687,8 +904,7 @@ int pl_serve_reset_stats(void* server) {
   std::lock_guard<std::mutex> lk(S->mu);
   S->lat.clear();
   S->sets_done = 0;
-  S->waves_launched = 0;
-  S->inflight_max = 0;
+  S->running_max = 0;
   S->t_first = S->t_last = 0;
   S->arena.peak = S->arena.used;
   return PL_OK;

@@ -18,6 +18,8 @@ Cases:
   k256     batched form, k = 256 (thread-block-cluster engine).
   gram     on-the-fly Gram blocks, Phi 2048 x 16384 N(0, 1/2048), k = 128.
   uneven   binned launch over the uneven-k stream (P(k) ~ 1/k, k <= 256).
+  gather   the gather alone (pl_gather_blocks), k = 64 on the k64 matrix,
+           default 100,000 sets (A[S,S] blocks written to HBM).
 """
 from __future__ import annotations
 
@@ -32,7 +34,7 @@ sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", required=True,
-                    choices=["k64", "plain64", "k128", "k192", "k256", "gram", "uneven"])
+                    choices=["k64", "plain64", "k128", "k192", "k256", "gram", "uneven", "gather"])
     ap.add_argument("--nsets", type=int, default=0)
     ap.add_argument("--launches", type=int, default=2)
     ap.add_argument("--variant", type=int, default=-2,
@@ -44,7 +46,8 @@ def main(argv=None) -> int:
     import workloads as W
     from paralanczos_b200 import api
     if a.variant >= -1:
-        kb = {"k64": 64, "plain64": 64, "k128": 128, "k192": 192, "k256": 256, "gram": 128, "uneven": 0}[a.case]
+        kb = {"k64": 64, "plain64": 64, "k128": 128, "k192": 192, "k256": 256, "gram": 128, "uneven": 0,
+              "gather": 64}[a.case]
         b = next(i for i in range(api.num_bins()) if api.bin_kmax(i) >= kb) if kb else 0
         api.tune_set(b, a.variant)
         print(f"bin {b}: variant {a.variant} ({api.tune_describe(b, max(a.variant, 0))[1]})")
@@ -61,7 +64,14 @@ def main(argv=None) -> int:
     else:
         n = W.C2["n"]
         A = torch.from_numpy(np.array(W.c2_matrix()[1])).to(dev)
-        if a.case == "uneven":
+        if a.case == "gather":
+            k = 64
+            nsets = a.nsets or 100_000
+            idx = api.gen_sets(1, 0, nsets, n, k)
+            blocks = api.gather_blocks(A, idx, k)
+            for _ in range(a.launches):
+                api.gather_blocks(A, idx, k, out=blocks)
+        elif a.case == "uneven":
             nsets = a.nsets or 100_000
             off_h, idx_h = api.gen_stream_host(1, 0, nsets, n, kdist=1)
             idx = torch.from_numpy(idx_h).to(dev)

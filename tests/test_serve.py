@@ -2,9 +2,13 @@
 
 A request's result must not depend on what it is batched with: requests are
 solved alone and inside a mix of other matrices and k, and the results are
-compared bit for bit, and against pl_solve on the same sets.  Admission by
-the HBM budget, back-pressure of the pinned pool and per-set error reporting
-are checked through the public API.
+compared bit for bit, and against pl_solve on the same sets.  The batching
+runs in device-resident request loops (a CUDA graph per loop under a
+conditional WHILE node); a loop with nothing to do ends itself after a
+bounded idle wait and is launched again by the next request.  Admission by
+the HBM budget (which covers all of the server's device memory),
+back-pressure of the pinned pool and per-set error reporting are checked
+through the public API.
 """
 import threading
 
@@ -53,7 +57,7 @@ def test_alone_and_in_a_mix_are_bit_identical(mats):
     rng = np.random.default_rng(0)
     k0 = 48
     S0 = _sets(rng, 100, 1024, k0)
-    with Server(budget_bytes=256 << 20, host_pool_bytes=256 << 20) as srv:
+    with Server(budget_bytes=1 << 30, host_pool_bytes=256 << 20) as srv:
         ids = [srv.add_matrix(A) for A in mats]
         alone = srv.wait(srv.submit(ids[1], S0, k0), len(S0))
         # a burst of mixed requests with the same request in the middle
@@ -90,7 +94,7 @@ def test_results_match_dsyev(mats):
     from paralanczos_b200.api import Server
     rng = np.random.default_rng(1)
     A = mats[0].cpu().numpy().astype(np.float64)
-    with Server(budget_bytes=64 << 20, host_pool_bytes=64 << 20) as srv:
+    with Server(budget_bytes=1 << 30, host_pool_bytes=64 << 20) as srv:
         mid = srv.add_matrix(mats[0])
         for k in (8, 64, 128, 192):
             S = _sets(rng, 20, 1024, k)
@@ -106,21 +110,57 @@ def test_admission_respects_the_budget(mats):
     from paralanczos_b200._lib import PLError
     from paralanczos_b200.api import Server
     rng = np.random.default_rng(2)
-    budget = 600_000
-    with Server(budget_bytes=budget, host_pool_bytes=64 << 20, max_waves=3) as srv:
+    budget = 384 << 20
+    with Server(budget_bytes=budget, host_pool_bytes=1 << 30, max_waves=1) as srv:
+        st0 = srv.stats()
+        # every device byte of the server (arena, wave staging, scratch) is
+        # inside the budget; what is left for indices is the arena
+        assert st0["device_bytes"] <= budget
+        arena = int(st0["arena_bytes"])
         mid = srv.add_matrix(mats[0])
-        # each request's indices take 200 KB of arena: at most two fit at once
-        batch = [_sets(rng, 500, 1024, 100) for _ in range(8)]
+        # each request's indices take a little over a third of the arena: at
+        # most two fit at once, so admission waits for completions
+        nsets = arena // 3 // (4 * 100) + 1
+        batch = [_sets(rng, nsets, 1024, 100) for _ in range(5)]
         ids = [srv.submit(mid, S, 100) for S in batch]
-        res = [srv.wait(i, 500) for i in ids]
+        res = [srv.wait(i, nsets, 300.0) for i in ids]
         st = srv.stats()
-        assert st["arena_peak"] <= budget
-        assert st["waves"] >= 4
-        for S, r in zip(batch, res):
+        assert st["arena_peak"] <= arena
+        assert st["arena_peak"] >= 2 * nsets * 400
+        for S, r in zip(batch[:2], res[:2]):
             _same(r, _solve_direct(mats[0], S, 100))
         # a request that can never fit is refused up front
         with pytest.raises(PLError):
-            srv.submit(mid, _sets(rng, 3000, 1024, 64), 64)
+            srv.submit(mid, np.zeros(arena // 4 + 64, dtype=np.int32), 64)
+    # a budget that does not even hold the server's staging is refused
+    with pytest.raises(PLError):
+        Server(budget_bytes=8 << 20, host_pool_bytes=1 << 20)
+
+
+def test_idle_loop_ends_and_restarts(mats, monkeypatch):
+    """With nothing to do a request loop waits at most PL_SERVE_IDLE_MS on the
+    device and then ends (its graph finishes with status "idle"); the next
+    request launches it again and is served."""
+    import time
+
+    from paralanczos_b200.api import Server
+    monkeypatch.setenv("PL_SERVE_IDLE_MS", "5")
+    rng = np.random.default_rng(9)
+    with Server(budget_bytes=1 << 30, host_pool_bytes=64 << 20, max_waves=1) as srv:
+        mid = srv.add_matrix(mats[0])
+        S1 = _sets(rng, 50, 1024, 32)
+        r1 = srv.wait(srv.submit(mid, S1, 32), 50)
+        time.sleep(0.3)
+        st = srv.stats()
+        assert st["loop_launches"] >= 1
+        assert st["idle_exits"] == st["loop_launches"]
+        assert st["loops_running"] == 0
+        S2 = _sets(rng, 50, 1024, 32)
+        r2 = srv.wait(srv.submit(mid, S2, 32), 50)
+        st2 = srv.stats()
+        assert st2["loop_launches"] == st["loop_launches"] + 1
+        _same(r1, _solve_direct(mats[0], S1, 32))
+        _same(r2, _solve_direct(mats[0], S2, 32))
 
 
 def test_large_request_split_over_waves_is_exact(mats, monkeypatch):
@@ -133,7 +173,7 @@ def test_large_request_split_over_waves_is_exact(mats, monkeypatch):
     rng = np.random.default_rng(7)
     monkeypatch.setenv("PL_SERVE_WAVE_MS", "0.5")
     S = _sets(rng, 2000, 1024, 200)
-    with Server(budget_bytes=64 << 20, host_pool_bytes=64 << 20) as srv:
+    with Server(budget_bytes=1 << 30, host_pool_bytes=64 << 20) as srv:
         mid = srv.add_matrix(mats[0])
         r = srv.wait(srv.submit(mid, S, 200), len(S))
         assert srv.stats()["waves"] >= 20
@@ -141,7 +181,7 @@ def test_large_request_split_over_waves_is_exact(mats, monkeypatch):
     monkeypatch.delenv("PL_SERVE_WAVE_MS")
     big = _sets(rng, 1500, 2048, 500)
     small = _sets(rng, 5, 2048, 16)
-    with Server(budget_bytes=64 << 20, host_pool_bytes=64 << 20) as srv:
+    with Server(budget_bytes=1 << 30, host_pool_bytes=64 << 20) as srv:
         mid = srv.add_matrix(mats[2])
         rb = srv.submit(mid, big, 500)
         time.sleep(0.005)
@@ -155,7 +195,7 @@ def test_large_request_split_over_waves_is_exact(mats, monkeypatch):
 def test_pinned_pool_backpressure(mats):
     from paralanczos_b200.api import Server
     rng = np.random.default_rng(3)
-    with Server(budget_bytes=64 << 20, host_pool_bytes=300_000) as srv:
+    with Server(budget_bytes=1 << 30, host_pool_bytes=300_000) as srv:
         mid = srv.add_matrix(mats[0])
         S = _sets(rng, 400, 1024, 64)      # ~110 KB of pinned staging each
         first = [srv.try_submit(mid, S, 64) for _ in range(4)]
@@ -173,7 +213,7 @@ def test_bad_index_and_bad_arguments(mats):
     from paralanczos_b200._lib import PLError
     from paralanczos_b200.api import Server
     rng = np.random.default_rng(4)
-    with Server(budget_bytes=16 << 20, host_pool_bytes=16 << 20) as srv:
+    with Server(budget_bytes=1 << 30, host_pool_bytes=16 << 20) as srv:
         mid = srv.add_matrix(mats[0])
         S = _sets(rng, 5, 1024, 16)
         S[3, 2] = 5000
@@ -191,7 +231,7 @@ def test_bad_index_and_bad_arguments(mats):
 def test_many_client_threads(mats):
     from paralanczos_b200.api import Server
     errors = []
-    with Server(budget_bytes=128 << 20, host_pool_bytes=128 << 20) as srv:
+    with Server(budget_bytes=1 << 30, host_pool_bytes=128 << 20) as srv:
         ids = [srv.add_matrix(A) for A in mats]
 
         def client(seed):
