@@ -233,10 +233,10 @@ cudaError_t launch_large(const MatrixF32& M, const SetSource& src, const SetOutp
   return cudaGetLastError();
 }
 
-template <int KB, int CS, int NTC, int RPT = 1, bool SPLIT = false>
+template <int KB, int CS, int NTC, int RPT = 1>
 cudaError_t launch_cluster(const MatrixF32& M, const SetSource& src, const SetOutputs& out,
                            long long nitems, void*, cudaStream_t st, bool prep) {
-  auto kern = k_cluster_solve<KB, CS, NTC, RPT, SPLIT>;
+  auto kern = k_cluster_solve<KB, CS, NTC, RPT>;
   const size_t dsm = sizeof(ClusterSmem<KB, CS, NTC>);
   static int maxcl = [&] {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
@@ -311,13 +311,6 @@ struct Variant {
     "cluster KB=" #KB " CS=" #CS " NTC=" #NTC " RPT=" #RPT,                                     \
         {launch_cluster<KB, CS, NTC, RPT>, nullptr}, {scratch_none, scratch_none}               \
   }
-// the same with each per-step cluster exchange split into arrive ... wait
-// around independent work (cluster_solve_set_split)
-#define CLUSTERS(KB, CS, NTC, RPT)                                                            \
-  Variant {                                                                                     \
-    "cluster split KB=" #KB " CS=" #CS " NTC=" #NTC " RPT=" #RPT,                               \
-        {launch_cluster<KB, CS, NTC, RPT, true>, nullptr}, {scratch_none, scratch_none}         \
-  }
 #define LARGE(KM) \
   Variant {                                                                             \
     "large KM=" #KM " CTA=256", {launch_large<KM, false>, launch_large<KM, true>},      \
@@ -338,13 +331,11 @@ const std::vector<Variant>& variants(int b) {
       {CLUSTER(192, 2, 384), LARGE(256), CLUSTER(192, 4, 192), CLUSTER(192, 1, 384), CLUSTER(192, 1, 768),
        CLUSTERR(192, 1, 384, 2), CLUSTERR(192, 1, 384, 4)},
       {CLUSTER(256, 2, 512), LARGE(256), CLUSTER(256, 4, 256), CLUSTER(256, 8, 256), CLUSTER(256, 2, 256),
-       CLUSTERR(256, 2, 256, 2), CLUSTERR(256, 2, 256, 4), CLUSTERS(256, 2, 256, 4), CLUSTERS(256, 2, 256, 2),
-       CLUSTERS(256, 4, 256, 2)},
+       CLUSTERR(256, 2, 256, 2), CLUSTERR(256, 2, 256, 4)},
       {CLUSTER(384, 4, 384), LARGE(512), CLUSTER(384, 8, 192), CLUSTER(384, 6, 256), CLUSTERR(384, 6, 256, 2),
-       CLUSTERR(384, 6, 256, 4), CLUSTERR(384, 4, 384, 4), CLUSTERS(384, 4, 384, 4),
-       CLUSTERS(384, 6, 256, 2)},
+       CLUSTERR(384, 6, 256, 4), CLUSTERR(384, 4, 384, 4)},
       {CLUSTER(512, 8, 256), LARGE(512), CLUSTER(512, 8, 512), CLUSTERR(512, 8, 256, 2),
-       CLUSTERR(512, 8, 256, 4), CLUSTERS(512, 8, 256, 2), CLUSTERS(512, 8, 256, 4)},
+       CLUSTERR(512, 8, 256, 4)},
   };
   return v[b];
 }

@@ -108,41 +108,6 @@ __device__ __forceinline__ double cluster_sum(double x, ClusterSmem<KB, CS, NTC>
   }
 }
 
-// Split cluster barrier: arrive (release: this thread's earlier shared and
-// distributed-shared-memory accesses are ordered before it) ... wait
-// (acquire).  Work placed between the two overlaps the exchange.
-__device__ __forceinline__ void cluster_arrive() {
-  asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
-
-// First half of cluster_sum for CS > 1: the CTA's partial of x goes into
-// every peer's part[slot][rank]; the caller arrives at the cluster barrier,
-// and after its wait cluster_collect reads the sum (rank order, identical on
-// every rank).
-template <int KB, int CS, int NTC>
-__device__ __forceinline__ void cluster_post(double x, ClusterSmem<KB, CS, NTC>& sm, int slot,
-                                             cg::cluster_group& cl, int rank) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-  if ((threadIdx.x & 31) == 0) sm.red[threadIdx.x >> 5] = x;
-  __syncthreads();
-  if (threadIdx.x < CS) {
-    double s = sm.red[0];
-#pragma unroll
-    for (int i = 1; i < NTC / 32; ++i) s += sm.red[i];
-    cl.map_shared_rank(&sm, (unsigned)threadIdx.x)->part[slot][rank] = s;
-  }
-}
-
-template <int KB, int CS, int NTC>
-__device__ __forceinline__ double cluster_collect(const ClusterSmem<KB, CS, NTC>& sm, int slot) {
-  double s = sm.part[slot][0];
-#pragma unroll
-  for (int r = 1; r < CS; ++r) s += sm.part[slot][r];
-  return s;
-}
-
 template <int KB, int CS, int NTC, int RPT = 1>
 __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int* __restrict__ S,
                                                   int k, long long set, const SetOutputs& out,
@@ -416,368 +381,6 @@ __device__ __forceinline__ void cluster_solve_set(const MatrixF32& M, const int*
 #pragma unroll
             for (int ch = 0; ch < NCH; ++ch) {
               const int c = 4 * (g0 + TPR * ch);
-              dst[c] = Pr[q][2 * ch].x;
-              dst[c + 1] = Pr[q][2 * ch].y;
-              dst[c + 2] = Pr[q][2 * ch + 1].x;
-              dst[c + 3] = Pr[q][2 * ch + 1].y;
-            }
-          }
-        }
-      }
-      set_sync<CS>(cl);
-      float z[RPT];
-      double zp = 0.0;
-#pragma unroll
-      for (int q = 0; q < RPT; ++q) {
-        z[q] = sm.vb[nxt][r[q]];
-        zp = q == 0 ? (double)z[0] * (double)z[0] : fma((double)z[q], (double)z[q], zp);
-      }
-      const double zz = cluster_sum<KB, CS, NTC>(lead ? zp : 0.0, sm, 2, cl, rank);
-      if (t == 0 && rank == 0) sm.ab[j + 1].y = 0x1p-600;  // decoupled block (see sturm_count)
-      scp = sc;
-      sc = 1.0f / sqrtf((float)zz);
-      bprev = 0.f;
-#pragma unroll
-      for (int q = 0; q < RPT; ++q) v[q] = z[q] * sc;
-    }
-    const int old_prv = prv;
-    prv = cur;
-    cur = nxt;
-    nxt = old_prv;
-  }
-  set_sync<CS>(cl);  // every rank done with the step loop before T is read
-
-  // ---- extremes on rank 0: warp 0 lambda_min, warp 1 lambda_max, 33-way -----
-  if (rank == 0) {
-    if (status & SET_NONFINITE) {
-      if (t == 0) write_failed(out, set, 0, 0, status);
-    } else {
-      double glo = 1e300, ghi = -1e300;
-      if (t < 64) {
-        for (int i = t & 31; i < k; i += 32) {
-          const double rad = (i > 0 ? sqrt(sm.ab[i].y) : 0.0) + (i + 1 < k ? sqrt(sm.ab[i + 1].y) : 0.0);
-          glo = fmin(glo, sm.ab[i].x - rad);
-          ghi = fmax(ghi, sm.ab[i].x + rad);
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          glo = fmin(glo, __shfl_xor_sync(0xffffffffu, glo, o));
-          ghi = fmax(ghi, __shfl_xor_sync(0xffffffffu, ghi, o));
-        }
-        const double pad = 0x1p-51 * fmax(fabs(glo), fabs(ghi)) + 1e-300;
-        const double e = multisect_warp(sm.ab, k, glo - pad, ghi + pad, t < 32 ? 1 : k);
-        if ((t & 31) == 0) sm.part[2][t >> 5] = e;
-      }
-      __syncthreads();
-      if (t == 0) {
-        const double lmin = sm.part[2][0], lmax = sm.part[2][1];
-        if (out.lmin) out.lmin[set] = lmin;
-        if (out.lmax) out.lmax[set] = lmax;
-        if (out.delta) out.delta[set] = fmax(1.0 - lmin, lmax - 1.0);
-        if (out.err) out.err[set] = status;
-      }
-    }
-  }
-  set_sync<CS>(cl);  // rank 0's reads of T and part[] precede the next set's writes
-}
-
-// The same Lanczos step on a multi-CTA cluster with the two per-step
-// exchanges split into arrive ... wait, so that work which does not need the
-// exchanged data runs while it is in flight:
-//   exchange 1 (rows of y = A v_j, alpha partials): the rank-1 update
-//     P_j = P_{j-1} - v_j v_j^T (it needs only v_j, known everywhere);
-//   exchange 2 (rows of w, ||w||^2 partials): the part of the next matvec
-//     A w over the columns of the CTA's own rows (its own rows of w are in
-//     its own shared memory after a CTA barrier).
-// For the second overlap each thread's float4 column chunks are taken in an
-// order rotated by rank * OWN, so that the chunks in the CTA's own column
-// block come first (OWN per thread, a compile-time count); a shape whose
-// column block is not a whole number of a thread's chunks (OWN = 0) overlaps
-// only the first exchange.  Bitwise identical scalars on every rank (partials
-// summed in rank order), every branch cluster-uniform.
-template <int KB, int CS, int NTC, int RPT>
-__device__ __forceinline__ void cluster_solve_set_split(const MatrixF32& M, const int* __restrict__ S, int k,
-                                                        long long set, const SetOutputs& out,
-                                                        ClusterSmem<KB, CS, NTC>& sm, cg::cluster_group& cl,
-                                                        int rank) {
-  using C = CfgC<KB, CS, NTC, RPT>;
-  constexpr int R = C::R, RS = C::RS, TPR = C::TPR, CPT = C::CPT, NCH = C::NCH;
-  constexpr int OWN = ((R / 4) % TPR == 0) ? (R / 4) / TPR : 0;
-  static_assert(CS > 1, "multi-CTA sets only");
-  const int t = threadIdx.x;
-  const int ls = t / TPR;
-  int r[RPT];
-#pragma unroll
-  for (int q = 0; q < RPT; ++q) r[q] = rank * R + ls + q * RS;
-  const int g0 = t % TPR;
-  const bool lead = g0 == 0;
-  const unsigned rmask = (TPR == 32) ? 0xffffffffu : (((1u << TPR) - 1u) << ((t & 31) / TPR * TPR));
-  const int rot = OWN ? rank * OWN : 0;
-  // first column of the thread's chunk in position ch
-  auto col = [&](int ch) { return 4 * (g0 + TPR * ((ch + rot) % NCH)); };
-
-  // ---- indices (every CTA keeps the full set), validation -------------------
-  const SetMatrix SM = set_matrix(M, set);
-  bool bad = false;
-  for (int c = t; c < KB; c += NTC) {
-    int v = 0;
-    if (c < k) {
-      v = SM.index(S, c);
-      bad |= (v < 0) | (v >= SM.n);
-    }
-    sm.idx[c] = (c < k && v >= 0 && v < SM.n) ? v : 0;
-  }
-  const double badsum = cluster_sum<KB, CS, NTC>(__any_sync(0xffffffffu, bad) ? 1.0 : 0.0, sm, 3, cl, rank);
-  if (badsum != 0.0) {
-    if (rank == 0 && t == 0) write_failed(out, set, 0, 0, SET_BAD_INDEX);
-    set_sync<CS>(cl);
-    return;
-  }
-
-  // ---- gather own rows of A_S into shared memory; P = I ----------------------
-  float4* __restrict__ my = sm.A + t;  // chunk (q, ch) at my[(q * NCH + ch) * NTC]
-  float2 Pr[RPT][CPT / 2];
-  double fro = 0.0;
-#pragma unroll
-  for (int q = 0; q < RPT; ++q) {
-    const bool rv = r[q] < k;
-    const float* __restrict__ arow = SM.A + (size_t)sm.idx[r[q]] * (size_t)SM.lda;
-#pragma unroll
-    for (int ch = 0; ch < NCH; ++ch) {
-      const int c0 = col(ch);
-      float e[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int c = c0 + u;
-        e[u] = (rv && c < k) ? __ldg(arow + sm.idx[c]) : 0.f;
-        fro += (double)e[u] * (double)e[u];
-      }
-      my[(q * NCH + ch) * NTC] = make_float4(e[0], e[1], e[2], e[3]);
-      Pr[q][2 * ch] = make_float2((rv && c0 == r[q]) ? 1.f : 0.f, (rv && c0 + 1 == r[q]) ? 1.f : 0.f);
-      Pr[q][2 * ch + 1] = make_float2((rv && c0 + 2 == r[q]) ? 1.f : 0.f, (rv && c0 + 3 == r[q]) ? 1.f : 0.f);
-    }
-  }
-  const double fro2 = cluster_sum<KB, CS, NTC>(fro, sm, 2, cl, rank);
-  const double tau2 = (32.0 * (double)kEps32) * (32.0 * (double)kEps32) * fro2;
-
-  const float v0 = (float)(1.0 / sqrt((double)k));
-  float v[RPT];
-#pragma unroll
-  for (int q = 0; q < RPT; ++q) v[q] = r[q] < k ? v0 : 0.f;
-  for (int c = t; c < KB; c += NTC) {
-    sm.vb[0][c] = c < k ? v0 : 0.f;
-    sm.vb[1][c] = 0.f;
-  }
-  if (t == 0) sm.ab[0].y = 0.0;
-  float sc = 1.f, scp = 0.f, bprev = 0.f;
-  int status = 0;
-  int cur = 0, prv = 1, nxt = 2;
-  float2 oa[RPT], ob[RPT];  // own-column part of the next A w (unnormalised)
-  bool own_ready = false;
-  __syncthreads();
-
-  for (int j = 0; j < k; ++j) {
-    // ---- y = A v_j: the chunks not already done during the last exchange
-    float2 ya[RPT], yb[RPT];
-#pragma unroll
-    for (int q = 0; q < RPT; ++q) {
-      ya[q] = own_ready ? oa[q] : make_float2(0.f, 0.f);
-      yb[q] = own_ready ? ob[q] : make_float2(0.f, 0.f);
-    }
-    if (!own_ready) {
-#pragma unroll
-      for (int ch = 0; ch < OWN; ++ch) {
-        const float4 b4 = *reinterpret_cast<const float4*>(&sm.vb[cur][col(ch)]);
-#pragma unroll
-        for (int q = 0; q < RPT; ++q) {
-          const float4 a4 = my[(q * NCH + ch) * NTC];
-          ya[q] = __ffma2_rn(make_float2(a4.x, a4.y), make_float2(b4.x, b4.y), ya[q]);
-          yb[q] = __ffma2_rn(make_float2(a4.z, a4.w), make_float2(b4.z, b4.w), yb[q]);
-        }
-      }
-    }
-#pragma unroll
-    for (int ch = OWN; ch < NCH; ++ch) {
-      const float4 b4 = *reinterpret_cast<const float4*>(&sm.vb[cur][col(ch)]);
-#pragma unroll
-      for (int q = 0; q < RPT; ++q) {
-        const float4 a4 = my[(q * NCH + ch) * NTC];
-        ya[q] = __ffma2_rn(make_float2(a4.x, a4.y), make_float2(b4.x, b4.y), ya[q]);
-        yb[q] = __ffma2_rn(make_float2(a4.z, a4.w), make_float2(b4.z, b4.w), yb[q]);
-      }
-    }
-    float y[RPT];
-    double ap = 0.0;
-#pragma unroll
-    for (int q = 0; q < RPT; ++q) {
-      y[q] = ((ya[q].x + ya[q].y) + (yb[q].x + yb[q].y)) * sc;
-#pragma unroll
-      for (int o = TPR / 2; o > 0; o >>= 1) y[q] += __shfl_xor_sync(rmask, y[q], o);
-      ap = q == 0 ? (double)v[0] * (double)y[0] : fma((double)v[q], (double)y[q], ap);
-    }
-    if (lead) {
-#pragma unroll
-      for (int p = 0; p < CS; ++p) {
-        ClusterSmem<KB, CS, NTC>* peer = cl.map_shared_rank(&sm, (unsigned)p);
-#pragma unroll
-        for (int q = 0; q < RPT; ++q) peer->yb[r[q]] = y[q];
-      }
-    }
-    cluster_post<KB, CS, NTC>(lead ? ap : 0.0, sm, 0, cl, rank);
-    cluster_arrive();
-    // ---- exchange 1 in flight: P_j = P_{j-1} - v_j v_j^T
-    {
-      float2 nc[RPT];
-#pragma unroll
-      for (int q = 0; q < RPT; ++q) {
-        const float cq = -v[q] * sc;
-        nc[q] = make_float2(cq, cq);
-      }
-#pragma unroll
-      for (int ch = 0; ch < NCH; ++ch) {
-        const float4 b4 = *reinterpret_cast<const float4*>(&sm.vb[cur][col(ch)]);
-#pragma unroll
-        for (int q = 0; q < RPT; ++q) {
-          Pr[q][2 * ch] = __ffma2_rn(nc[q], make_float2(b4.x, b4.y), Pr[q][2 * ch]);
-          Pr[q][2 * ch + 1] = __ffma2_rn(nc[q], make_float2(b4.z, b4.w), Pr[q][2 * ch + 1]);
-        }
-      }
-    }
-    cluster_wait();
-    const double alpha = cluster_collect<KB, CS, NTC>(sm, 0);
-    const float af = (float)alpha;
-
-    // w~ = y - alpha v_j - beta_j v_{j-1}, every element formed locally
-    for (int c = t; c < KB; c += NTC)
-      sm.wb[c] = fmaf(-af, sc * sm.vb[cur][c], fmaf(-bprev, scp * sm.vb[prv][c], sm.yb[c]));
-    __syncthreads();
-
-    // ---- w = P_j w~ over the owned row slices
-    float2 wa[RPT], wc[RPT];
-#pragma unroll
-    for (int q = 0; q < RPT; ++q) {
-      wa[q] = make_float2(0.f, 0.f);
-      wc[q] = make_float2(0.f, 0.f);
-    }
-#pragma unroll
-    for (int ch = 0; ch < NCH; ++ch) {
-      const float4 x4 = *reinterpret_cast<const float4*>(&sm.wb[col(ch)]);
-#pragma unroll
-      for (int q = 0; q < RPT; ++q) {
-        wa[q] = __ffma2_rn(Pr[q][2 * ch], make_float2(x4.x, x4.y), wa[q]);
-        wc[q] = __ffma2_rn(Pr[q][2 * ch + 1], make_float2(x4.z, x4.w), wc[q]);
-      }
-    }
-    float w[RPT];
-    double bp = 0.0;
-#pragma unroll
-    for (int q = 0; q < RPT; ++q) {
-      w[q] = (wa[q].x + wa[q].y) + (wc[q].x + wc[q].y);
-#pragma unroll
-      for (int o = TPR / 2; o > 0; o >>= 1) w[q] += __shfl_xor_sync(rmask, w[q], o);
-      bp = q == 0 ? (double)w[0] * (double)w[0] : fma((double)w[q], (double)w[q], bp);
-    }
-    if (lead) {
-#pragma unroll
-      for (int p = 0; p < CS; ++p) {
-        ClusterSmem<KB, CS, NTC>* peer = cl.map_shared_rank(&sm, (unsigned)p);
-#pragma unroll
-        for (int q = 0; q < RPT; ++q) peer->vb[nxt][r[q]] = w[q];
-      }
-    }
-    cluster_post<KB, CS, NTC>(lead ? bp : 0.0, sm, 1, cl, rank);
-    cluster_arrive();
-    // ---- exchange 2 in flight: the own-column part of A w
-    if constexpr (OWN > 0) {
-      __syncthreads();  // the CTA's own rows of w are in its vb[nxt]
-#pragma unroll
-      for (int q = 0; q < RPT; ++q) {
-        oa[q] = make_float2(0.f, 0.f);
-        ob[q] = make_float2(0.f, 0.f);
-      }
-#pragma unroll
-      for (int ch = 0; ch < OWN; ++ch) {
-        const float4 b4 = *reinterpret_cast<const float4*>(&sm.vb[nxt][col(ch)]);
-#pragma unroll
-        for (int q = 0; q < RPT; ++q) {
-          const float4 a4 = my[(q * NCH + ch) * NTC];
-          oa[q] = __ffma2_rn(make_float2(a4.x, a4.y), make_float2(b4.x, b4.y), oa[q]);
-          ob[q] = __ffma2_rn(make_float2(a4.z, a4.w), make_float2(b4.z, b4.w), ob[q]);
-        }
-      }
-      own_ready = true;
-    }
-    cluster_wait();
-    const double b2v = cluster_collect<KB, CS, NTC>(sm, 1);
-    if (t == 0 && rank == 0) {
-      sm.ab[j].x = alpha;
-      if (j + 1 < k) sm.ab[j + 1].y = b2v;
-    }
-    if (!isfinite(alpha) || !isfinite(b2v)) {
-      status |= SET_NONFINITE;
-      break;
-    }
-    if (j + 1 == k) break;
-    if (b2v > tau2) {
-      const float bf = sqrtf((float)b2v);
-      scp = sc;
-      sc = 1.0f / bf;
-      bprev = bf;
-#pragma unroll
-      for (int q = 0; q < RPT; ++q) v[q] = w[q] * sc;
-    } else {
-      // Breakdown: restart from the column of P with the largest diagonal
-      // (cluster-wide argmax, ties to the smaller row), published into vb[nxt].
-      status |= SET_BREAKDOWN;
-      own_ready = false;  // the next matvec is of the restart vector
-      unsigned long long kk = 0ull;
-#pragma unroll
-      for (int q = 0; q < RPT; ++q) {
-        float d = -1.f;
-#pragma unroll
-        for (int ch = 0; ch < NCH; ++ch) {
-          const int c = col(ch);
-          if (c == r[q]) d = Pr[q][2 * ch].x;
-          if (c + 1 == r[q]) d = Pr[q][2 * ch].y;
-          if (c + 2 == r[q]) d = Pr[q][2 * ch + 1].x;
-          if (c + 3 == r[q]) d = Pr[q][2 * ch + 1].y;
-        }
-        if (r[q] < k && d >= -0.5f) {  // this thread owns column r[q] of row r[q]
-          d = fmaxf(d, 0.f);
-          const unsigned long long kq =
-              ((unsigned long long)__float_as_uint(d) << 32) | (unsigned)(0x7fffffff - r[q]);
-          kk = kq > kk ? kq : kk;
-        }
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long y2 = __shfl_xor_sync(0xffffffffu, kk, o);
-        kk = y2 > kk ? y2 : kk;
-      }
-      if ((t & 31) == 0) sm.red[t >> 5] = __longlong_as_double((long long)kk);
-      __syncthreads();
-      if (t < CS) {
-        unsigned long long m = 0;
-        for (int i = 0; i < NTC / 32; ++i) {
-          const unsigned long long y2 = (unsigned long long)__double_as_longlong(sm.red[i]);
-          m = y2 > m ? y2 : m;
-        }
-        cl.map_shared_rank(&sm, (unsigned)t)->key[rank] = m;
-      }
-      set_sync<CS>(cl);
-      unsigned long long best = 0;
-#pragma unroll
-      for (int q = 0; q < CS; ++q) best = sm.key[q] > best ? sm.key[q] : best;
-      const int mrow = 0x7fffffff - (int)(best & 0xffffffffu);
-#pragma unroll
-      for (int q = 0; q < RPT; ++q) {
-        if (r[q] == mrow) {
-#pragma unroll
-          for (int p = 0; p < CS; ++p) {
-            float* dst = cl.map_shared_rank(&sm, (unsigned)p)->vb[nxt];
-#pragma unroll
-            for (int ch = 0; ch < NCH; ++ch) {
-              const int c = col(ch);
               dst[c] = Pr[q][2 * ch].x;
               dst[c + 1] = Pr[q][2 * ch].y;
               dst[c + 2] = Pr[q][2 * ch + 1].x;

@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(256, 1)
 // Large-k batched form on thread-block clusters (pl_cluster.cuh): persistent,
 // one set per cluster of CS CTAs at a time.
 // ---------------------------------------------------------------------------
-template <int KB, int CS, int NTC, int RPT = 1, bool SPLIT = false>
+template <int KB, int CS, int NTC, int RPT = 1>
 __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(NTC, 1)
     k_cluster_solve(MatrixF32 M, SetSource src, SetOutputs out) {
   extern __shared__ __align__(16) float dsm[];
@@ -262,10 +262,7 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(NTC, 1)
       if (rank == 0 && threadIdx.x == 0) write_failed(out, set, off, 0, SET_BAD_K);
       continue;
     }
-    if constexpr (CS == 1 || !SPLIT)
-      cluster_solve_set<KB, CS, NTC, RPT>(M, src.idx + off, k, set, out, sm, cl, rank);
-    else
-      cluster_solve_set_split<KB, CS, NTC, RPT>(M, src.idx + off, k, set, out, sm, cl, rank);
+    cluster_solve_set<KB, CS, NTC, RPT>(M, src.idx + off, k, set, out, sm, cl, rank);
   }
 }
 
@@ -355,12 +352,12 @@ __global__ void k_f64_to_f32(const double* __restrict__ in, float* __restrict__ 
 // are read (k(k+1)/2 random 4-byte loads per set: each one is its own L1
 // request and 32-byte sector, the cost of a random gather) and each is
 // written to (i, j) and (j, i).  One set per CTA at a time, in 64 x 64 tiles
-// (I <= J): a diagonal tile is read as its upper triangle and mirrored in
-// shared memory; an off-diagonal tile is read whole, written as tile (I, J)
-// straight from registers and as tile (J, I) through a shared-memory
-// transpose.  Warp w of the 8 owns tile rows w, w + 8, ...; lane l columns
-// l and l + 32; every load of a tile is issued before the first is used, and
-// every global write is a coalesced 128-byte row segment.  The blocks are
+// (I <= J): a diagonal tile is read as its upper triangle (enumerated over all
+// 256 threads) and mirrored in shared memory; an off-diagonal tile is read
+// whole (warp w owns tile rows w, w + 8, ..., lane l columns l and l + 32),
+// written as tile (I, J) straight from registers and as tile (J, I) through a
+// shared-memory transpose.  Every load of a tile is issued before the first is
+// used, and every global write is a coalesced 128-byte row segment.  The blocks are
 // written and the indices read with streaming (evict-first) accesses, so that
 // they do not push A out of L2, where its random elements are found.  err[s] =
 // SET_BAD_INDEX for an index outside [0, n) (its block is left as zeros).
@@ -370,34 +367,51 @@ __device__ __forceinline__ void gather_tile(const float* __restrict__ A, long lo
                                             int I, int J, float* __restrict__ out, float (*T)[kGTile + 1]) {
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int r0 = I * kGTile, c0 = J * kGTile;
-  const bool diag = I == J;
-  float e[kGRows][2];
+  if (I == J) {
+    // The tile's upper triangle, enumerated so that every lane loads: rows p
+    // and kk-1-p (kk = the tile's valid order rounded up to even) together
+    // hold kk+1 upper elements; element e of the kk/2 pairs goes to thread
+    // e % 256, at most 9 per thread, all loads issued before the stores.
+    constexpr int kPer = (kGTile / 2 * (kGTile + 1) + 255) / 256;
+    const int kt = k - r0 < kGTile ? k - r0 : kGTile;
+    const int kk = (kt + 1) & ~1, per = kk + 1, total = (kk / 2) * per;
+    float e[kPer];
+    int rc[kPer];  // (row << 8) | col within the tile, -1 for none
 #pragma unroll
-  for (int u = 0; u < kGRows; ++u) {
-    const int r = w + 8 * u;
-    const bool rv = r0 + r < k;
-    const float* __restrict__ row = A + (size_t)sidx[rv ? r0 + r : 0] * (size_t)lda;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int c = lane + 32 * h;
-      const bool v = rv && c0 + c < k && (!diag || c >= r);
-      e[u][h] = v ? __ldg(row + sidx[c0 + c]) : 0.f;
+    for (int u = 0; u < kPer; ++u) {
+      const int q = threadIdx.x + 256 * u;
+      int r = -1, c = -1;
+      if (q < total) {
+        const int p = q / per, i = q - p * per;
+        const bool first = i < kk - p;
+        r = first ? p : kk - 1 - p;
+        c = first ? p + i : i - 1;  // c >= r
+      }
+      const bool v = r >= 0 && r < kt && c < kt;
+      rc[u] = v ? (r << 8) | c : -1;
+      e[u] = v ? __ldg(A + (size_t)sidx[r0 + r] * (size_t)lda + sidx[r0 + c]) : 0.f;
     }
-  }
-  if (diag) {
 #pragma unroll
-    for (int u = 0; u < kGRows; ++u) {
-      const int r = w + 8 * u;
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int c = lane + 32 * h;
-        if (c >= r) {
-          T[r][c] = e[u][h];
-          T[c][r] = e[u][h];
-        }
+    for (int u = 0; u < kPer; ++u) {
+      if (rc[u] >= 0) {
+        const int r = rc[u] >> 8, c = rc[u] & 255;
+        T[r][c] = e[u];
+        T[c][r] = e[u];
       }
     }
   } else {
+    float e[kGRows][2];
+#pragma unroll
+    for (int u = 0; u < kGRows; ++u) {
+      const int r = w + 8 * u;
+      const bool rv = r0 + r < k;
+      const float* __restrict__ row = A + (size_t)sidx[rv ? r0 + r : 0] * (size_t)lda;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int c = lane + 32 * h;
+        e[u][h] = (rv && c0 + c < k) ? __ldg(row + sidx[c0 + c]) : 0.f;
+      }
+    }
 #pragma unroll
     for (int u = 0; u < kGRows; ++u) {
       const int r = w + 8 * u;
