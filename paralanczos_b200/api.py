@@ -309,7 +309,7 @@ class Server:
     PL_EBUSY when the pinned pool is full); ``wait`` returns its results as a
     dict of numpy arrays plus ``latency_s`` (submit to completion)."""
 
-    def __init__(self, budget_bytes: int = 1 << 30, host_pool_bytes: int = 1 << 30, max_waves: int = 3):
+    def __init__(self, budget_bytes: int = 1 << 30, host_pool_bytes: int = 1 << 30, max_waves: int = 4):
         self._h = C.c_void_p()
         self._mats = []   # keep the registered tensors alive
         check(lib().pl_serve_create(int(budget_bytes), int(host_pool_bytes), int(max_waves),

@@ -377,15 +377,24 @@ __device__ __forceinline__ void gather_tile(const float* __restrict__ A, long lo
     const int kk = (kt + 1) & ~1, per = kk + 1, total = (kk / 2) * per;
     float e[kPer];
     int rc[kPer];  // (row << 8) | col within the tile, -1 for none
+    // element q = threadIdx.x + 256 u is (pair p, position i); p and i are
+    // stepped by 256 = dp * per + di instead of dividing per element
+    const int dp = 256 / per, di = 256 - dp * per;
+    int p = threadIdx.x / per, i = threadIdx.x - p * per;
 #pragma unroll
     for (int u = 0; u < kPer; ++u) {
       const int q = threadIdx.x + 256 * u;
       int r = -1, c = -1;
       if (q < total) {
-        const int p = q / per, i = q - p * per;
         const bool first = i < kk - p;
         r = first ? p : kk - 1 - p;
         c = first ? p + i : i - 1;  // c >= r
+      }
+      p += dp;
+      i += di;
+      if (i >= per) {
+        i -= per;
+        ++p;
       }
       const bool v = r >= 0 && r < kt && c < kt;
       rc[u] = v ? (r << 8) | c : -1;
@@ -437,11 +446,121 @@ __device__ __forceinline__ void gather_tile(const float* __restrict__ A, long lo
   __syncthreads();
 }
 
+// k <= 64 (one diagonal tile per set), software-pipelined across the CTA's
+// sets: the loads of set s + G are in flight while set s's block is written
+// out of shared memory, and the indices of set s + 2 G are loaded (into a
+// register of thread c < k) a set earlier still.  Each thread's share of the
+// triangle -- at most 9 (row, column) pairs -- depends only on k and is
+// worked out once.
+__device__ __forceinline__ void gather_small(const float* __restrict__ A, int n, long long lda,
+                                             const int* __restrict__ idx, long long nsets, int k,
+                                             float* __restrict__ blocks, int* __restrict__ err, int* sidx,
+                                             float (*T)[kGTile + 1]) {
+  constexpr int kPer = (kGTile / 2 * (kGTile + 1) + 255) / 256;
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  const int kk = (k + 1) & ~1, per = kk + 1, total = (kk / 2) * per;
+  int rc[kPer];  // (row << 8) | col, -1 for none
+  {
+    const int dp = 256 / per, di = 256 - dp * per;
+    int p = tid / per, i = tid - p * per;
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      int r = -1, c = -1;
+      if (tid + 256 * u < total) {
+        const bool first = i < kk - p;
+        r = first ? p : kk - 1 - p;
+        c = first ? p + i : i - 1;
+      }
+      p += dp;
+      i += di;
+      if (i >= per) {
+        i -= per;
+        ++p;
+      }
+      rc[u] = (r >= 0 && r < k && c < k) ? (r << 8) | c : -1;
+    }
+  }
+  const long long G = gridDim.x, kb = (long long)k * k;
+  long long s = blockIdx.x;
+  if (s >= nsets) return;
+  // the first set's indices, the second set's into a register
+  int buf = 0;
+  int bad;
+  {
+    int b = 0;
+    if (tid < k) {
+      const int v = __ldcs(idx + s * k + tid);
+      b = (v < 0) | (v >= n);
+      sidx[tid] = v;
+    }
+    bad = __syncthreads_or(b);
+  }
+  int nidx = 0;
+  if (tid < k && s + G < nsets) nidx = __ldcs(idx + (s + G) * k + tid);
+  float e[kPer];
+#pragma unroll
+  for (int u = 0; u < kPer; ++u) {
+    const int r = rc[u] >> 8, c = rc[u] & 255;
+    e[u] = (!bad && rc[u] >= 0) ? __ldg(A + (size_t)sidx[r] * (size_t)lda + sidx[c]) : 0.f;
+  }
+  for (; s < nsets; s += G) {
+    const long long sn = s + G;
+    // this set's triangle into T (mirrored)
+    if (!bad) {
+#pragma unroll
+      for (int u = 0; u < kPer; ++u) {
+        if (rc[u] >= 0) {
+          const int r = rc[u] >> 8, c = rc[u] & 255;
+          T[r][c] = e[u];
+          T[c][r] = e[u];
+        }
+      }
+    }
+    // the next set's indices (already in registers) into the other buffer;
+    // the barrier also publishes T
+    int* nb = sidx + (buf ^ 1) * kGTile;
+    int bn = 0;
+    if (tid < k && sn < nsets) {
+      bn = (nidx < 0) | (nidx >= n);
+      nb[tid] = nidx;
+    }
+    bn = __syncthreads_or(bn);
+    if (tid < k && sn + G < nsets) nidx = __ldcs(idx + (sn + G) * k + tid);
+    // the next set's loads in flight ...
+    if (sn < nsets && !bn) {
+#pragma unroll
+      for (int u = 0; u < kPer; ++u) {
+        const int r = rc[u] >> 8, c = rc[u] & 255;
+        e[u] = rc[u] >= 0 ? __ldg(A + (size_t)nb[r] * (size_t)lda + nb[c]) : 0.f;
+      }
+    }
+    // ... while this set's block goes out
+    float* __restrict__ out = blocks + s * kb;
+#pragma unroll
+    for (int u = 0; u < kGRows; ++u) {
+      const int r = w + 8 * u;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int c = lane + 32 * h;
+        if (r < k && c < k) __stcs(out + (size_t)r * k + c, bad ? 0.f : T[r][c]);
+      }
+    }
+    if (tid == 0 && err) err[s] = bad ? SET_BAD_INDEX : SET_OK;
+    __syncthreads();  // T and this set's index buffer are free
+    bad = bn;
+    buf ^= 1;
+  }
+}
+
 __global__ void __launch_bounds__(256, 4) k_gather_blocks(const float* __restrict__ A, int n, long long lda,
                                                       const int* __restrict__ idx, long long nsets, int k,
                                                       float* __restrict__ blocks, int* __restrict__ err) {
   __shared__ int sidx[512];
   __shared__ float T[kGTile][kGTile + 1];
+  if (k <= kGTile) {
+    gather_small(A, n, lda, idx, nsets, k, blocks, err, sidx, T);
+    return;
+  }
   const long long kk = (long long)k * k;
   const int nt = (k + kGTile - 1) / kGTile;
   for (long long s = blockIdx.x; s < nsets; s += gridDim.x) {

@@ -11,28 +11,30 @@
 //   * the host admits queued requests in arrival order while their indices
 //     fit the device arena, uploads them, and then publishes one descriptor
 //     per request into a descriptor ring in mapped host memory;
-//   * a request loop runs on the device: one CUDA graph per loop whose body
-//     sits under a conditional WHILE node -- a planning kernel, an expansion
-//     kernel, the binned launch of the batched form (device counting sort by
-//     k, one persistent kernel per k bin), and a completion kernel -- and
-//     repeats without the host.  Each pass the planning kernel absorbs new
-//     descriptors into the loop's table of active requests and forms the next
-//     "wave" of about PL_SERVE_WAVE_MS (default 20) ms of estimated GPU work:
-//     the oldest unfinished request gets up to PL_SERVE_OLDEST_SHARE (default
-//     0.9) of it, then the requests with the least work left fill the rest, so
-//     large requests are split over waves and small ones that arrive behind
-//     them go out in the next wave.  The expansion kernel lays the wave's sets
-//     out as one CSR batch (indices copied from the arena, per-set matrix ids);
-//     the completion kernel writes each set's results straight into its
-//     request's mapped host buffers and, with the last set of a request, its
-//     completion flag;
-//   * when a loop has nothing to do, its planning kernel polls the ring
+//   * request loops run on the device, up to four: each is one CUDA graph whose
+//     body sits under a conditional WHILE node -- a planning kernel, an
+//     expansion kernel, the binned launch of the batched form (device counting
+//     sort by k, one persistent kernel per k bin), and a completion kernel --
+//     and repeats without the host.  The loops share one table of active
+//     requests in device memory: each pass a loop's planning kernel absorbs new
+//     descriptors from the ring (claiming each with a compare-and-swap), scans
+//     the table with a whole CTA, and forms its next "wave" of about
+//     PL_SERVE_WAVE_MS (default 20) ms of estimated GPU work -- the oldest
+//     unfinished request gets up to PL_SERVE_OLDEST_SHARE (default 0.9) of it,
+//     then the requests with the least work left fill the rest -- claiming the
+//     sets with atomic adds, so two loops never take the same set and no kernel
+//     waits on another.  With several loops, several waves are in flight and
+//     their kernels overlap (one wave's tail is filled by the next), in one
+//     global oldest-first order: large requests are split over waves and are
+//     not stretched by sharing, small ones that arrive behind them go out in
+//     the next wave.  The expansion kernel lays a wave's sets out as one CSR
+//     batch (indices copied from the arena, per-set matrix ids); the completion
+//     kernel writes each set's results straight into its request's mapped host
+//     buffers and, with the last set of a request, its completion flag;
+//   * when a loop finds nothing to do, its planning kernel polls the ring
 //     (bounded by %globaltimer, PL_SERVE_IDLE_MS, default 20 ms) and then ends
 //     the loop (the graph finishes, status "idle"); the host launches it again
 //     when the next descriptor is published.  Every device wait is bounded;
-//   * requests are spread over up to four loops by k (small k apart from large
-//     k), so small requests never wait behind a long large-k wave, and the
-//     loops' kernels overlap on the GPU;
 //   * all device memory of the server -- arena, wave staging, kernel scratch,
 //     tables -- is allocated at creation inside budget_bytes.
 // A set's result does not depend on what else is in its wave: each set is
@@ -65,8 +67,7 @@ namespace serve {
 
 constexpr int kMaxMatrices = 64;
 constexpr int kMaxBinsS = 16;
-constexpr int kMaxLoops = 4;
-constexpr int kRing = 4096;             // descriptor ring entries per loop
+constexpr int kRing = 4096;  // descriptor ring entries
 
 double now_s() {
   using namespace std::chrono;
@@ -122,10 +123,10 @@ struct Arena {
 };
 
 struct LoopArgs {
-  Ctl* ctl;
-  const RingDesc* ring;
-  DevReq* tab;
-  Plan* plan;
+  Ctl* ctl;              // mapped
+  const RingDesc* ring;  // mapped
+  Shared* sh;            // device, shared by the loops
+  Plan* plan;            // device, this loop's
   const int* arena;
   int* widx;
   long long* woff;
@@ -137,6 +138,7 @@ struct LoopArgs {
   cudaGraphConditionalHandle cond;
   unsigned long long idle_ns;
   double wave_us, oldest_share;
+  int loop;
 };
 
 __device__ __forceinline__ long long ld_acquire_sys(const long long* p) {
@@ -145,49 +147,103 @@ __device__ __forceinline__ long long ld_acquire_sys(const long long* p) {
   return v;
 }
 
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
 __device__ __forceinline__ void st_release_sys(long long* p, long long v) {
   asm volatile("st.release.sys.global.s64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-// Planning (one thread): retire finished requests, absorb new descriptors,
-// wait for work at most idle_ns, form the next wave or end the loop.
-__global__ void k_loop_plan(LoopArgs a) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  Plan& P = *a.plan;
-  int n = 0;
-  for (int i = 0; i < P.nact; ++i) {
-    const int s = P.act[i];
-    if (a.tab[s].done < a.tab[s].nsets) P.act[n++] = s;
+__device__ __forceinline__ void st_release_gpu(int* p, int v) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// New descriptors into the shared table (one thread).  Each ring entry is
+// claimed by exactly one planner (compare-and-swap on the shared cursor); the
+// request becomes visible to the scans by a release store of `live` after its
+// fields.
+__device__ void absorb(const LoopArgs& a) {
+  const long long tail = ld_acquire_sys(&a.ctl->tail);
+  for (int it = 0; it < kRing; ++it) {
+    const unsigned long long h = *(volatile unsigned long long*)&a.sh->head;
+    if ((long long)h >= tail) break;
+    if (atomicCAS(&a.sh->head, h, h + 1) != h) continue;
+    const RingDesc d = a.ring[h % kRing];
+    DevReq& r = a.sh->tab[d.slot];
+    r.id = d.id;
+    r.nsets = d.nsets;
+    r.next = 0;
+    r.done = 0;
+    r.arena_off = d.arena_off;
+    r.lmin = d.lmin;
+    r.lmax = d.lmax;
+    r.delta = d.delta;
+    r.err = d.err;
+    r.mat = d.mat;
+    r.k = d.k;
+    st_release_gpu(&r.live, 1);
+    *(volatile long long*)&a.ctl->head = (long long)h + 1;
   }
-  P.nact = n;
+}
+
+// Planning (one CTA of 256 threads): absorb, scan the table for requests with
+// sets left, wait for work at most idle_ns, then form this loop's next wave
+// (thread 0) or end the loop.
+__global__ void __launch_bounds__(256) k_loop_plan(LoopArgs a) {
+  __shared__ Cand cand[kSlots];
+  __shared__ int nc, decision;
   const unsigned long long t0 = globaltimer();
   for (;;) {
-    const long long tail = ld_acquire_sys(&a.ctl->tail);
-    while (P.head < tail && P.nact < kSlots) {
-      const RingDesc d = a.ring[P.head % kRing];
-      a.tab[d.slot] = DevReq{d.id, d.nsets, 0, 0, d.arena_off, d.lmin, d.lmax, d.delta, d.err, d.mat, d.k};
-      P.act[P.nact++] = d.slot;
-      ++P.head;
+    if (threadIdx.x == 0) {
+      absorb(a);
+      nc = 0;
     }
-    *(volatile long long*)&a.ctl->head = P.head;
-    const int stop = *(volatile int*)&a.ctl->stop;
-    bool work = false;
-    for (int i = 0; i < P.nact && !work; ++i) work = a.tab[P.act[i]].next < a.tab[P.act[i]].nsets;
-    if (work && !stop) break;
-    if (stop || globaltimer() - t0 > a.idle_ns) {
-      P.nsets = 0;
-      P.npieces = 0;
-      *(volatile int*)&a.ctl->status = stop ? 3 : 2;
-      cudaGraphSetConditional(a.cond, 0);
+    __syncthreads();
+    for (int s = threadIdx.x; s < kSlots; s += blockDim.x) {
+      const DevReq& r = a.sh->tab[s];
+      if (ld_acquire_gpu(&r.live)) {
+        const long long nx = *(volatile const long long*)&r.next;
+        if (nx < r.nsets) {
+          const int i = atomicAdd(&nc, 1);
+          cand[i] = Cand{r.id, r.nsets - nx, s, r.k};
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int stop = *(volatile int*)&a.ctl->stop;
+      decision = (nc > 0 && !stop) ? 1 : ((stop || globaltimer() - t0 > a.idle_ns) ? 2 : 0);
+      if (decision == 0) __nanosleep(2000);
+    }
+    __syncthreads();
+    if (decision == 1) break;
+    if (decision == 2) {
+      if (threadIdx.x == 0) {
+        a.plan->nsets = 0;
+        a.plan->npieces = 0;
+        *(volatile int*)&a.ctl->status[a.loop] = *(volatile int*)&a.ctl->stop ? 3 : 2;
+        cudaGraphSetConditional(a.cond, 0);
+      }
       return;
     }
-    __nanosleep(2000);
   }
+  if (threadIdx.x != 0) return;
+  auto claim = [&](int slot, long long want, long long* first) -> long long {
+    DevReq& r = a.sh->tab[slot];
+    const long long old = (long long)atomicAdd(reinterpret_cast<unsigned long long*>(&r.next),
+                                               (unsigned long long)want);
+    if (old >= r.nsets) return 0;
+    *first = old;
+    return want < r.nsets - old ? want : r.nsets - old;
+  };
   long long ns = 0;
-  P.npieces = form_wave(a.tab, P.act, P.nact, a.wave_us, a.oldest_share, P.pieces, &ns);
-  P.nsets = ns;
-  *(volatile long long*)&a.ctl->waves = *(volatile long long*)&a.ctl->waves + 1;
-  cudaGraphSetConditional(a.cond, 1);
+  a.plan->npieces = form_wave(cand, nc, a.wave_us, a.oldest_share, a.plan->pieces, &ns, claim);
+  a.plan->nsets = ns;
+  *(volatile long long*)&a.ctl->waves[a.loop] = *(volatile long long*)&a.ctl->waves[a.loop] + 1;
+  cudaGraphSetConditional(a.cond, 1);  // an empty wave (claims lost to other loops) plans again
 }
 
 // The wave as one CSR batch: a warp per set copies its indices from the arena.
@@ -204,7 +260,7 @@ __global__ void __launch_bounds__(256) k_loop_expand(LoopArgs a) {
     }
     const Piece pc = P.pieces[lo];
     const long long j = s - pc.set0, pos = pc.first + j, off = pc.idx0 + j * pc.k;
-    const DevReq& r = a.tab[pc.slot];
+    const DevReq& r = a.sh->tab[pc.slot];
     const int* __restrict__ src = a.arena + r.arena_off + pos * pc.k;
     for (int i = lane; i < pc.k; i += 32) a.widx[off + i] = src[i];
     if (lane == 0) {
@@ -218,14 +274,15 @@ __global__ void __launch_bounds__(256) k_loop_expand(LoopArgs a) {
 }
 
 // Results into the requests' mapped host buffers; the last set of a request
-// publishes its completion flag after every result of it is visible.
+// retires it (live = 0) and then publishes its completion flag, after every
+// result of it is visible to the host.
 __global__ void __launch_bounds__(256) k_loop_finish(LoopArgs a) {
   const long long ns = a.plan->nsets;
   for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < ns;
        s += (long long)gridDim.x * blockDim.x) {
     const int slot = a.wslot[s];
     const long long pos = a.wpos[s];
-    DevReq& r = a.tab[slot];
+    DevReq& r = a.sh->tab[slot];
     r.lmin[pos] = a.wres[s];
     r.lmax[pos] = a.wres[kWaveSets + s];
     r.delta[pos] = a.wres[2 * kWaveSets + s];
@@ -233,6 +290,7 @@ __global__ void __launch_bounds__(256) k_loop_finish(LoopArgs a) {
     __threadfence_system();
     const unsigned long long prev = atomicAdd(reinterpret_cast<unsigned long long*>(&r.done), 1ull);
     if ((long long)prev + 1 == r.nsets) {
+      *(volatile int*)&r.live = 0;
       __threadfence_system();
       st_release_sys(&a.ctl->done_id[slot], r.id);
     }
@@ -254,7 +312,7 @@ struct Request {
   int state = PENDING;
   int status = PL_OK;
   size_t dev_off = 0, dev_len = 0;  // arena block holding the indices on the device
-  int loop = 0, slot = -1;
+  int slot = -1;
 };
 
 size_t req_dev_bytes(long long nsets, int k) { return a256(sizeof(int) * (size_t)nsets * k); }
@@ -264,11 +322,8 @@ size_t req_host_bytes(long long nsets, int k) {
 }
 
 struct Loop {
-  Ctl* ctl = nullptr;  // mapped: host and device view are the same address (UVA)
-  RingDesc* ring = nullptr;
-  DevReq* tab = nullptr;
   Plan* plan = nullptr;
-  char* dmem = nullptr;  // one device allocation: tab, plan, wave staging, scratch
+  char* dmem = nullptr;  // one device allocation: plan, wave staging, scratch
   LoopArgs args{};
   void* scratch = nullptr;
   cudaStream_t st = nullptr, cap = nullptr;
@@ -277,9 +332,6 @@ struct Loop {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   bool running = false;
-  long long published = 0;
-  std::vector<int> free_slots;
-  std::vector<Request*> live;  // published, not complete
   long long launches = 0, idle_exits = 0;
 };
 
@@ -292,6 +344,14 @@ struct Server {
   char* d_pool = nullptr;  // the pool's device address
   MatrixRef* d_mats = nullptr;
   std::vector<MatrixRef> mats;
+  Shared* sh = nullptr;    // device: the shared request table
+  Ctl* ctl = nullptr;      // mapped
+  RingDesc* ring = nullptr;  // mapped
+  Ctl* ctl_d = nullptr;
+  RingDesc* ring_d = nullptr;
+  long long published = 0;
+  std::vector<int> free_slots;
+  std::vector<Request*> live;  // published, not complete
   Loop loops[kMaxLoops];
   size_t fixed_bytes = 0, budget = 0;
   cudaStream_t up = nullptr;  // index uploads at admission
@@ -316,18 +376,9 @@ int cuda_fail(cudaError_t e) {
   return e == cudaErrorMemoryAllocation ? PL_ENOMEM : PL_ECUDA;
 }
 
-// Loop of a request: small k apart from large k (upper k of loop i).
-int loop_of(const Server& S, int k) {
-  static const int edges[kMaxLoops + 1][kMaxLoops] = {
-      {0}, {1 << 30}, {128, 1 << 30}, {64, 192, 1 << 30}, {32, 128, 256, 1 << 30}};
-  for (int i = 0; i < S.nloops; ++i)
-    if (k <= edges[S.nloops][i]) return i;
-  return S.nloops - 1;
-}
-
-// Device bytes of one loop (tables, wave staging, binned-launch scratch).
+// Device bytes of one loop (its wave, wave staging, binned-launch scratch).
 struct LoopLayout {
-  size_t tab, plan, widx, woff, wmat, wslot, wpos, wres, werr, scratch, total;
+  size_t plan, widx, woff, wmat, wslot, wpos, wres, werr, scratch, total;
 };
 LoopLayout loop_layout() {
   LoopLayout L;
@@ -337,7 +388,6 @@ LoopLayout loop_layout() {
     o += a256(n);
     return at;
   };
-  L.tab = take(sizeof(DevReq) * kSlots);
   L.plan = take(sizeof(Plan));
   L.widx = take(sizeof(int) * (size_t)kWaveIdx);
   L.woff = take(sizeof(long long) * (size_t)(kWaveSets + 1));
@@ -351,29 +401,18 @@ LoopLayout loop_layout() {
   return L;
 }
 
-// The loop's graph: WHILE(cond) { plan; expand; binned solve; finish }.
-int build_loop(Server& S, Loop& L) {
+// A loop's graph: WHILE(cond) { plan; expand; binned solve; finish }.
+int build_loop(Server& S, Loop& L, int li) {
   const LoopLayout lay = loop_layout();
   cudaError_t e;
   if ((e = cudaMalloc(&L.dmem, lay.total)) != cudaSuccess) return cuda_fail(e);
-  if ((e = cudaMemset(L.dmem, 0, lay.tab + lay.plan + sizeof(Plan))) != cudaSuccess) return cuda_fail(e);
-  if ((e = cudaHostAlloc(&L.ctl, sizeof(Ctl), cudaHostAllocMapped)) != cudaSuccess) return cuda_fail(e);
-  if ((e = cudaHostAlloc(&L.ring, sizeof(RingDesc) * kRing, cudaHostAllocMapped)) != cudaSuccess)
-    return cuda_fail(e);
-  memset(L.ctl, 0, sizeof(Ctl));
-  for (int i = 0; i < kSlots; ++i) L.ctl->done_id[i] = -1;
-  L.tab = (DevReq*)(L.dmem + lay.tab);
+  if ((e = cudaMemset(L.dmem + lay.plan, 0, sizeof(Plan))) != cudaSuccess) return cuda_fail(e);
   L.plan = (Plan*)(L.dmem + lay.plan);
   L.scratch = L.dmem + lay.scratch;
-  for (int i = kSlots - 1; i >= 0; --i) L.free_slots.push_back(i);
-  Ctl* ctl_d = nullptr;
-  RingDesc* ring_d = nullptr;
-  if ((e = cudaHostGetDevicePointer((void**)&ctl_d, L.ctl, 0)) != cudaSuccess) return cuda_fail(e);
-  if ((e = cudaHostGetDevicePointer((void**)&ring_d, L.ring, 0)) != cudaSuccess) return cuda_fail(e);
   LoopArgs& a = L.args;
-  a.ctl = ctl_d;
-  a.ring = ring_d;
-  a.tab = L.tab;
+  a.ctl = S.ctl_d;
+  a.ring = S.ring_d;
+  a.sh = S.sh;
   a.plan = L.plan;
   a.arena = (const int*)S.d_arena;
   a.widx = (int*)(L.dmem + lay.widx);
@@ -386,6 +425,7 @@ int build_loop(Server& S, Loop& L) {
   a.idle_ns = (unsigned long long)(S.idle_ms * 1e6);
   a.wave_us = S.wave_us;
   a.oldest_share = S.oldest_share;
+  a.loop = li;
   if ((e = cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaStreamCreateWithFlags(&L.cap, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaEventCreateWithFlags(&L.fork, cudaEventDisableTiming)) != cudaSuccess)
@@ -416,7 +456,7 @@ int build_loop(Server& S, Loop& L) {
   if ((e = cudaStreamBeginCaptureToGraph(L.cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
       cudaSuccess)
     return cuda_fail(e);
-  k_loop_plan<<<1, 32, 0, L.cap>>>(a);
+  k_loop_plan<<<1, 256, 0, L.cap>>>(a);
   k_loop_expand<<<sms * 4, 256, 0, L.cap>>>(a);
   MatrixF32 M{nullptr, 0, 0};
   M.mats = S.d_mats;
@@ -436,16 +476,16 @@ int build_loop(Server& S, Loop& L) {
   return PL_OK;
 }
 
-void fail_loop(Server& S, Loop& L, int status) {
+void fail_live(Server& S, int status) {
   const double t = now_s();
-  for (Request* r : L.live) {
+  for (Request* r : S.live) {
     r->state = FAILED;
     r->status = status;
     r->t_done = t;
     S.arena.release(r->dev_off, r->dev_len);
-    L.free_slots.push_back(r->slot);
+    S.free_slots.push_back(r->slot);
   }
-  L.live.clear();
+  S.live.clear();
 }
 
 void scheduler(Server* sp) {
@@ -456,61 +496,56 @@ void scheduler(Server* sp) {
     bool progressed = false;
     // ---- completions: flags written by the device loops
     const double t = now_s();
-    for (int li = 0; li < S.nloops; ++li) {
-      Loop& L = S.loops[li];
-      for (size_t i = 0; i < L.live.size();) {
-        Request* r = L.live[i];
-        if (*(volatile long long*)&L.ctl->done_id[r->slot] == r->id) {
-          r->state = DONE;
-          r->t_done = t;
-          S.lat.push_back(t - r->t_submit);
-          S.t_last = t;
-          S.sets_done += r->nsets;
-          S.arena.release(r->dev_off, r->dev_len);
-          L.free_slots.push_back(r->slot);
-          L.live[i] = L.live.back();
-          L.live.pop_back();
-          progressed = true;
-        } else {
-          ++i;
-        }
+    for (size_t i = 0; i < S.live.size();) {
+      Request* r = S.live[i];
+      if (*(volatile long long*)&S.ctl->done_id[r->slot] == r->id) {
+        r->state = DONE;
+        r->t_done = t;
+        S.lat.push_back(t - r->t_submit);
+        S.t_last = t;
+        S.sets_done += r->nsets;
+        S.arena.release(r->dev_off, r->dev_len);
+        S.free_slots.push_back(r->slot);
+        S.live[i] = S.live.back();
+        S.live.pop_back();
+        progressed = true;
+      } else {
+        ++i;
       }
     }
     if (progressed) S.cv_done.notify_all();
-    // ---- publication of the uploaded batch
+    // ---- publication of the uploaded batch (in arrival order)
     if (!S.uploading.empty() && cudaEventQuery(S.up_ev) == cudaSuccess) {
       for (Request* r : S.uploading) {
-        Loop& L = S.loops[r->loop];
-        RingDesc& d = L.ring[L.published % kRing];
+        RingDesc& d = S.ring[S.published % kRing];
         const size_t nres = (size_t)r->nsets;
         double* res = (double*)(S.d_pool + ((char*)r->h_res - S.h_pool));
         int* err = (int*)(S.d_pool + ((char*)r->h_err - S.h_pool));
         d = RingDesc{r->id, r->nsets, (long long)(r->dev_off / sizeof(int)), res, res + nres, res + 2 * nres,
                      err, r->slot, r->mat, r->k, 0};
         std::atomic_thread_fence(std::memory_order_release);
-        ++L.published;
-        *(volatile long long*)&L.ctl->tail = L.published;
+        ++S.published;
+        *(volatile long long*)&S.ctl->tail = S.published;
         r->state = PUBLISHED;
-        L.live.push_back(r);
+        S.live.push_back(r);
       }
       S.uploading.clear();
       progressed = true;
     }
-    // ---- admission: arrival order, while the indices fit the arena and the
-    //      request's loop has a free slot and ring room
+    // ---- admission: arrival order, while the indices fit the arena, a slot
+    //      is free and the ring has room (a margin for entries being copied)
     if (S.uploading.empty()) {
       while (!S.pending.empty()) {
         Request* r = S.pending.front();
-        Loop& L = S.loops[r->loop];
-        if (L.free_slots.empty()) break;
-        if (L.published - *(volatile long long*)&L.ctl->head >= kRing) break;
+        if (S.free_slots.empty()) break;
+        if (S.published + (long long)S.uploading.size() - *(volatile long long*)&S.ctl->head >= kRing - 64) break;
         size_t off = 0;
         const size_t b = req_dev_bytes(r->nsets, r->k);
         if (!S.arena.alloc(b, &off)) break;
         r->dev_off = off;
         r->dev_len = b;
-        r->slot = L.free_slots.back();
-        L.free_slots.pop_back();
+        r->slot = S.free_slots.back();
+        S.free_slots.pop_back();
         r->state = UPLOADING;
         cudaError_t e = cudaMemcpyAsync(S.d_arena + off, r->h_idx, sizeof(int) * (size_t)r->nsets * r->k,
                                         cudaMemcpyHostToDevice, S.up);
@@ -524,7 +559,7 @@ void scheduler(Server* sp) {
         progressed = true;
       }
     }
-    // ---- the device loops: notice ended ones, (re)launch where work waits
+    // ---- the device loops: notice ended ones, (re)launch while work is live
     int running = 0;
     for (int li = 0; li < S.nloops; ++li) {
       Loop& L = S.loops[li];
@@ -532,22 +567,21 @@ void scheduler(Server* sp) {
         const cudaError_t q = cudaStreamQuery(L.st);
         if (q == cudaSuccess) {
           L.running = false;
-          if (*(volatile int*)&L.ctl->status == 2) ++L.idle_exits;
+          if (*(volatile int*)&S.ctl->status[li] == 2) ++L.idle_exits;
         } else if (q != cudaErrorNotReady) {
           api_note_cuda(q);
           L.running = false;
-          fail_loop(S, L, PL_ECUDA);
+          fail_live(S, PL_ECUDA);
           S.cv_done.notify_all();
         }
       }
-      if (!L.running && !L.live.empty()) {
-        *(volatile int*)&L.ctl->stop = 0;
-        *(volatile int*)&L.ctl->status = 1;
+      if (!L.running && !S.live.empty()) {
+        *(volatile int*)&S.ctl->status[li] = 1;
         std::atomic_thread_fence(std::memory_order_release);
         const cudaError_t e = cudaGraphLaunch(L.exec, L.st);
         if (e != cudaSuccess) {
           api_note_cuda(e);
-          fail_loop(S, L, PL_ECUDA);
+          fail_live(S, PL_ECUDA);
           S.cv_done.notify_all();
         } else {
           L.running = true;
@@ -559,9 +593,7 @@ void scheduler(Server* sp) {
     }
     S.running_max = std::max(S.running_max, running);
     if (!progressed) {
-      bool busy = !S.uploading.empty();
-      for (int li = 0; li < S.nloops; ++li) busy |= !S.loops[li].live.empty();
-      if (busy) {
+      if (!S.uploading.empty() || !S.live.empty()) {
         lk.unlock();
         std::this_thread::sleep_for(std::chrono::microseconds(20));
         lk.lock();
@@ -581,9 +613,9 @@ int destroy(Server* S) {
   S->cv_work.notify_all();
   if (S->th.joinable()) S->th.join();
   cudaSetDevice(S->dev);
+  if (S->ctl) *(volatile int*)&S->ctl->stop = 1;  // a running loop leaves at its next poll
   for (int li = 0; li < kMaxLoops; ++li) {
     Loop& L = S->loops[li];
-    if (L.ctl) *(volatile int*)&L.ctl->stop = 1;  // a running loop leaves at its next poll
     if (L.st) cudaStreamSynchronize(L.st);
     if (L.exec) cudaGraphExecDestroy(L.exec);
     if (L.graph) cudaGraphDestroy(L.graph);
@@ -595,8 +627,6 @@ int destroy(Server* S) {
     if (L.cap) cudaStreamDestroy(L.cap);
     if (L.fork) cudaEventDestroy(L.fork);
     if (L.dmem) cudaFree(L.dmem);
-    if (L.ctl) cudaFreeHost(L.ctl);
-    if (L.ring) cudaFreeHost(L.ring);
   }
   if (S->up) cudaStreamSynchronize(S->up);
   if (S->up) cudaStreamDestroy(S->up);
@@ -604,6 +634,9 @@ int destroy(Server* S) {
   for (auto& kv : S->reqs) delete kv.second;
   if (S->d_arena) cudaFree(S->d_arena);
   if (S->d_mats) cudaFree(S->d_mats);
+  if (S->sh) cudaFree(S->sh);
+  if (S->ctl) cudaFreeHost(S->ctl);
+  if (S->ring) cudaFreeHost(S->ring);
   if (S->h_pool) cudaFreeHost(S->h_pool);
   delete S;
   return PL_OK;
@@ -622,7 +655,8 @@ int pl_serve_create(long long budget_bytes, long long host_pool_bytes, int max_w
     return PL_EINVAL;
   *server = nullptr;
   const int nloops = std::min(max_waves, kMaxLoops);
-  const size_t fixed = nloops * loop_layout().total + a256(sizeof(MatrixRef) * kMaxMatrices);
+  const size_t fixed =
+      nloops * loop_layout().total + a256(sizeof(MatrixRef) * kMaxMatrices) + a256(sizeof(Shared));
   if ((size_t)budget_bytes < fixed + (1u << 20)) return PL_EINVAL;  // no room for any indices
   Server* S = new Server();
   cudaGetDevice(&S->dev);
@@ -642,14 +676,20 @@ int pl_serve_create(long long budget_bytes, long long host_pool_bytes, int max_w
   cudaError_t e;
   if ((e = cudaMalloc(&S->d_arena, arena)) != cudaSuccess ||
       (e = cudaMalloc(&S->d_mats, sizeof(MatrixRef) * kMaxMatrices)) != cudaSuccess ||
-      (e = cudaHostAlloc(&S->h_pool, (size_t)host_pool_bytes, cudaHostAllocMapped)) != cudaSuccess) {
+      (e = cudaMalloc(&S->sh, sizeof(Shared))) != cudaSuccess ||
+      (e = cudaMemset(S->sh, 0, sizeof(Shared))) != cudaSuccess ||
+      (e = cudaHostAlloc(&S->ctl, sizeof(Ctl), cudaHostAllocMapped)) != cudaSuccess ||
+      (e = cudaHostAlloc(&S->ring, sizeof(RingDesc) * kRing, cudaHostAllocMapped)) != cudaSuccess ||
+      (e = cudaHostAlloc(&S->h_pool, (size_t)host_pool_bytes, cudaHostAllocMapped)) != cudaSuccess ||
+      (e = cudaHostGetDevicePointer((void**)&S->d_pool, S->h_pool, 0)) != cudaSuccess ||
+      (e = cudaHostGetDevicePointer((void**)&S->ctl_d, S->ctl, 0)) != cudaSuccess ||
+      (e = cudaHostGetDevicePointer((void**)&S->ring_d, S->ring, 0)) != cudaSuccess) {
     destroy(S);
     return cuda_fail(e);
   }
-  if ((e = cudaHostGetDevicePointer((void**)&S->d_pool, S->h_pool, 0)) != cudaSuccess) {
-    destroy(S);
-    return cuda_fail(e);
-  }
+  memset(S->ctl, 0, sizeof(Ctl));
+  for (int i = 0; i < kSlots; ++i) S->ctl->done_id[i] = -1;
+  for (int i = kSlots - 1; i >= 0; --i) S->free_slots.push_back(i);
   S->arena.init(arena);
   S->pool.init((size_t)host_pool_bytes);
   if ((e = cudaStreamCreateWithFlags(&S->up, cudaStreamNonBlocking)) != cudaSuccess ||
@@ -658,7 +698,7 @@ int pl_serve_create(long long budget_bytes, long long host_pool_bytes, int max_w
     return cuda_fail(e);
   }
   for (int li = 0; li < nloops; ++li) {
-    const int rc = build_loop(*S, S->loops[li]);
+    const int rc = build_loop(*S, S->loops[li], li);
     if (rc) {
       destroy(S);
       return rc;
@@ -701,7 +741,6 @@ int pl_serve_submit(void* server, int matrix_id, const int* idx, long long nsets
   r->mat = matrix_id;
   r->k = k;
   r->nsets = nsets;
-  r->loop = loop_of(*S, k);
   r->host_off = hoff;
   r->host_len = hb;
   char* hp = S->h_pool + hoff;
@@ -767,7 +806,7 @@ int pl_serve_stats(void* server, double* out, int nout) {
   int running = 0;
   for (int li = 0; li < S->nloops; ++li) {
     const Loop& L = S->loops[li];
-    waves += *(volatile long long*)&L.ctl->waves;
+    waves += *(volatile long long*)&S->ctl->waves[li];
     launches += L.launches;
     idle += L.idle_exits;
     running += L.running ? 1 : 0;

@@ -1,7 +1,9 @@
-// Host-side check of the serving loop's wave policy (pl_serve_plan.cuh): the
-// same form_wave the device planning kernel runs, driven wave after wave over
-// request tables, with its invariants checked.  Built and run by
-// tests/test_serve_plan.py (host code only: needs nvcc, no GPU).
+// Host-side check of the serving loops' wave policy (pl_serve_plan.cuh): the
+// same form_wave the device planning kernels run, driven wave after wave over
+// request tables -- by one planner, and by two planners whose claims
+// interleave the way two loops' atomic claims can -- with its invariants
+// checked.  Built and run by tests/test_serve_plan.py (host code only: needs
+// nvcc, no GPU).
 #include <stdio.h>
 #include <stdlib.h>
 
@@ -19,93 +21,131 @@ static unsigned long long next_rand() {
   return rng;
 }
 
-// Runs waves until every set is scheduled; returns the number of waves, or a
-// negative code on a broken invariant.
-static long long drive(std::vector<DevReq>& tab, std::vector<int>& act, double wave_us, double share) {
-  std::vector<Piece> pieces(kMaxPieces);
-  std::vector<long long> seen(tab.size(), 0);
+struct Table {
+  std::vector<long long> nsets, next, seen;
+  std::vector<int> k;
+};
+
+// Candidates as a scan sees them (remaining = nsets - next; stale views are
+// allowed: `lag` adds sets that another planner already claimed).
+static int scan(const Table& T, std::vector<Cand>& c, long long lag) {
+  int n = 0;
+  for (size_t s = 0; s < T.nsets.size(); ++s)
+    if (T.next[s] < T.nsets[s]) c[n++] = Cand{(long long)s, T.nsets[s] - T.next[s] + lag, (int)s, T.k[s]};
+  return n;
+}
+
+// Checks one wave; returns 0 or a negative code.
+static int check_wave(Table& T, const std::vector<Piece>& p, int np, long long ns) {
+  if (np < 0 || np > kMaxPieces || ns < 0 || ns > kWaveSets) return -2;
+  long long set0 = 0, idx0 = 0;
+  for (int i = 0; i < np; ++i) {
+    const Piece& pc = p[i];
+    if (pc.count < 1 || pc.set0 != set0 || pc.idx0 != idx0) return -3;  // contiguous wave layout
+    for (long long j = 0; j < pc.count; ++j)
+      if (pc.first + j >= T.nsets[pc.slot]) return -4;                 // never past the request
+    T.seen[pc.slot] += pc.count;
+    set0 += pc.count;
+    idx0 += pc.count * pc.k;
+  }
+  if (set0 != ns || idx0 > kWaveIdx) return -5;
+  return 0;
+}
+
+// Waves by `planners` planners taking turns (their claims interleave) until
+// every set is taken; returns the number of waves or a negative code.
+static long long drive(Table& T, double wave_us, double share, int planners) {
+  std::vector<Cand> c(T.nsets.size() + 1);
+  std::vector<Piece> p(kMaxPieces);
   long long waves = 0;
   for (;;) {
     bool work = false;
-    for (int s : act) work |= tab[s].next < tab[s].nsets;
+    for (size_t s = 0; s < T.nsets.size(); ++s) work |= T.next[s] < T.nsets[s];
     if (!work) break;
-    long long ns = 0;
-    const int np = form_wave(tab.data(), act.data(), (int)act.size(), wave_us, share, pieces.data(), &ns);
-    ++waves;
-    if (np < 1 || np > kMaxPieces) return -1;          // no progress / overflow
-    if (ns < 1 || ns > kWaveSets) return -2;
-    long long set0 = 0, idx0 = 0;
-    for (int p = 0; p < np; ++p) {
-      const Piece& pc = pieces[p];
-      if (pc.count < 1 || pc.set0 != set0 || pc.idx0 != idx0) return -3;  // contiguous wave layout
-      if (pc.first != seen[pc.slot]) return -4;                           // request order, no gap/overlap
-      seen[pc.slot] += pc.count;
-      set0 += pc.count;
-      idx0 += pc.count * pc.k;
+    // each planner scans first (so later ones see stale counts), then claims
+    std::vector<std::vector<Cand>> views(planners, c);
+    std::vector<int> nc(planners);
+    for (int q = 0; q < planners; ++q) nc[q] = scan(T, views[q], q ? 17 : 0);
+    bool any = false;
+    for (int q = 0; q < planners; ++q) {
+      auto claim = [&](int slot, long long want, long long* first) -> long long {
+        const long long old = T.next[slot];
+        T.next[slot] += want;  // like atomicAdd: may pass nsets
+        if (old >= T.nsets[slot]) return 0;
+        *first = old;
+        return want < T.nsets[slot] - old ? want : T.nsets[slot] - old;
+      };
+      long long ns = 0;
+      const int np = form_wave(views[q].data(), nc[q], wave_us, share, p.data(), &ns, claim);
+      ++waves;
+      const int rc = check_wave(T, p, np, ns);
+      if (rc) return rc;
+      any |= np > 0;
     }
-    if (set0 != ns || idx0 > kWaveIdx) return -5;
+    if (!any) return -1;  // nobody made progress while work was left
     if (waves > 10000000) return -6;
   }
-  for (size_t s = 0; s < tab.size(); ++s)
-    if (seen[s] != tab[s].nsets) return -7;             // every set exactly once
+  for (size_t s = 0; s < T.nsets.size(); ++s)
+    if (T.seen[s] != T.nsets[s]) return -7;  // every set exactly once
   return waves;
 }
 
-static DevReq req(long long nsets, int k) {
-  DevReq r{};
-  r.nsets = nsets;
-  r.k = k;
-  return r;
+static Table table(const std::vector<long long>& ns, const std::vector<int>& k) {
+  Table T;
+  T.nsets = ns;
+  T.k = k;
+  T.next.assign(ns.size(), 0);
+  T.seen.assign(ns.size(), 0);
+  return T;
 }
 
 int main() {
   int fails = 0;
-  // 1. indices fill the wave before the time budget: two large k = 100 requests
-  //    (the case where a full wave must end the selection)
-  {
-    std::vector<DevReq> tab = {req(228000, 100), req(228000, 100)};
-    std::vector<int> act = {0, 1};
-    const long long w = drive(tab, act, 20000.0, 0.9);
-    printf("index-full waves: %lld\n", w);
-    fails += w <= 0;
-  }
-  // 2. sets fill the wave: many tiny sets
-  {
-    std::vector<DevReq> tab = {req(300000, 8), req(5, 8)};
-    std::vector<int> act = {0, 1};
-    const long long w = drive(tab, act, 20000.0, 0.9);
-    printf("set-full waves: %lld\n", w);
-    fails += w <= 0;
-  }
-  // 3. pieces fill the wave: more requests than pieces
-  {
-    std::vector<DevReq> tab;
-    std::vector<int> act;
-    for (int i = 0; i < kSlots; ++i) {
-      tab.push_back(req(1 + i % 3, 8 + i % 7));
-      act.push_back(i);
+  for (int planners = 1; planners <= 3; ++planners) {
+    // indices fill the wave before its time budget (two large k = 100 requests)
+    {
+      Table T = table({228000, 228000}, {100, 100});
+      const long long w = drive(T, 20000.0, 0.9, planners);
+      printf("planners %d index-full waves: %lld\n", planners, w);
+      fails += w <= 0;
     }
-    const long long w = drive(tab, act, 1e9, 0.9);
-    printf("piece-full waves: %lld\n", w);
-    fails += w <= 0;
-  }
-  // 4. random tables, short and long waves, every share
-  for (int t = 0; t < 300; ++t) {
-    const int n = 1 + (int)(next_rand() % 200);
-    std::vector<DevReq> tab;
-    std::vector<int> act;
-    for (int i = 0; i < n; ++i) {
-      const int k = 1 + (int)(next_rand() % 512);
-      const long long ns = 1 + (long long)(next_rand() % 5000);
-      tab.push_back(req(ns, k));
-      act.push_back(i);
+    // sets fill the wave: many tiny sets
+    {
+      Table T = table({300000, 5}, {8, 8});
+      const long long w = drive(T, 20000.0, 0.9, planners);
+      printf("planners %d set-full waves: %lld\n", planners, w);
+      fails += w <= 0;
     }
-    const double wave = (t % 3 == 0) ? 50.0 : (t % 3 == 1) ? 20000.0 : 1e7;
-    const double share = 0.05 + 0.95 * (double)(next_rand() % 1000) / 999.0;
-    const long long w = drive(tab, act, wave, share);
-    if (w <= 0) {
-      printf("random table %d: invariant %lld broken\n", t, w);
-      ++fails;
+    // pieces fill the wave: more requests than pieces
+    {
+      std::vector<long long> ns;
+      std::vector<int> k;
+      for (int i = 0; i < kSlots; ++i) {
+        ns.push_back(1 + i % 3);
+        k.push_back(8 + i % 7);
+      }
+      Table T = table(ns, k);
+      const long long w = drive(T, 1e9, 0.9, planners);
+      printf("planners %d piece-full waves: %lld\n", planners, w);
+      fails += w <= 0;
+    }
+    // random tables, short and long waves, every share
+    for (int t = 0; t < 200; ++t) {
+      const int n = 1 + (int)(next_rand() % 200);
+      std::vector<long long> ns;
+      std::vector<int> k;
+      for (int i = 0; i < n; ++i) {
+        k.push_back(1 + (int)(next_rand() % 512));
+        ns.push_back(1 + (long long)(next_rand() % 5000));
+      }
+      Table T = table(ns, k);
+      const double wave = (t % 3 == 0) ? 50.0 : (t % 3 == 1) ? 20000.0 : 1e7;
+      const double share = 0.05 + 0.95 * (double)(next_rand() % 1000) / 999.0;
+      const long long w = drive(T, wave, share, planners);
+      if (w <= 0) {
+        printf("planners %d random table %d: invariant %lld broken\n", planners, t, w);
+        ++fails;
+      }
     }
   }
   printf("%s\n", fails ? "FAIL" : "OK");

@@ -17,7 +17,7 @@ def test_wave_policy_invariants(tmp_path):
     if not os.path.exists(nvcc):
         pytest.skip("nvcc absent")
     exe = tmp_path / "plan_check"
-    subprocess.run([nvcc, "-std=c++17", "-O1", os.path.join(HERE, "serve_plan_check.cu"), "-o", str(exe)],
+    subprocess.run([nvcc, "-std=c++17", "-O1", "--expt-relaxed-constexpr", os.path.join(HERE, "serve_plan_check.cu"), "-o", str(exe)],
                    check=True, capture_output=True, text=True, timeout=300)
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and r.stdout.strip().endswith("OK"), r.stdout + r.stderr
