@@ -139,3 +139,29 @@ def test_c3_per_k_vs_dsyev_and_oracle(c2_dev):
         print(f"C3 k={kv}: {len(sets)} sets; 200 vs dsyev max {e.max():.2e} p99 {np.percentile(e, 99):.2e}; "
               f"50 vs oracle max {eo.max():.2e}")
         assert e.max() <= RTOL and eo.max() <= RTOL
+
+
+@pytest.mark.parametrize("kind", ["gauss", "rademacher"])
+def test_c4_on_the_fly_gram_2000_sets(kind):
+    """C4: Phi 2048 x 16384 (seed 0, Gaussian or Rademacher), A never formed:
+    each A[S,S] = Phi_S^T Phi_S on the tensor cores (bf16 split products,
+    FP32 accumulation), then the Lanczos.  2,000 of the sets of k = 128 (the
+    first 2,000 of the generator's stream) against FP64 dsyev of the FP64 Gram
+    of the same FP32 frame columns; max and p99 printed."""
+    import torch
+    Phi = W.c4_frame(kind)
+    k, nsets = W.C4["k"], 2000
+    gf = api.GramFrame(torch.from_numpy(Phi).cuda())
+    idx = api.gen_sets(W.SEED_SETS, 0, nsets, W.C4["n"], k)
+    out = gf.solve(idx, k)
+    torch.cuda.synchronize()
+    r = {nm: t.cpu().numpy() for nm, t in out.items()}
+    assert _ok(r["err"])
+    S = idx.view(nsets, k).cpu().numpy()
+    errs = np.empty(nsets)
+    for s in range(nsets):
+        X = Phi[:, S[s]].astype(np.float64)
+        w = O.dsyev_eigs(X.T @ X)
+        errs[s] = max(abs(r["lmin"][s] - w[0]) / abs(w[0]), abs(r["lmax"][s] - w[-1]) / abs(w[-1]))
+    print(f"C4 {kind}: 2,000 sets k=128, vs dsyev max {errs.max():.2e} p99 {np.percentile(errs, 99):.2e}")
+    assert errs.max() <= RTOL

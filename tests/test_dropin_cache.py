@@ -4,7 +4,8 @@ The reference uploads the whole FP64 matrix on every call
 (ParaLanczos.cu:1845-1846).  Here calculate_subeigs3 and friends upload and
 convert it once (on the device) and reuse it while the caller passes the same
 matrix: same address, order and contents (a content hash of the host matrix
-per call).  Checked through the C ABI: the second call on an unchanged matrix
+per call, computed while a solve on the cached copy runs; a changed hash
+re-uploads and solves again).  Checked through the C ABI: the second call on an unchanged matrix
 is a cache hit with bit-identical results, a change of one element is a miss
 and is seen in the results, and a second matrix is a miss.
 """
