@@ -265,6 +265,33 @@ cudaError_t launch_cluster(const MatrixF32& M, const SetSource& src, const SetOu
   return cudaGetLastError();
 }
 
+// MINB > 0: launch-bounds form; MINB < 0: register cap of -MINB (k_sym_solve_r)
+template <int NB, int NW, int TPW, int MINB>
+cudaError_t launch_sym(const MatrixF32& M, const SetSource& src, const SetOutputs& out, long long nitems,
+                       void*, cudaStream_t st, bool prep) {
+  void (*kern)(MatrixF32, SetSource, SetOutputs);
+  if constexpr (MINB > 0)
+    kern = k_sym_solve<NB, NW, TPW, MINB>;
+  else
+    kern = k_sym_solve_r<NB, NW, TPW, -MINB>;
+  const size_t dsm = sizeof(SymSmem<NB, NW>);
+  static int occ = [&] {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
+    cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    return occupancy(kern, NW * 32, dsm);
+  }();
+  if (prep) {
+    cudaFuncAttributes fa;
+    return cudaFuncGetAttributes(&fa, kern);
+  }
+  const long long grid = grid_for(nitems, 1, occ);
+  if (verbosity() >= 2)
+    fprintf(stderr, "paralanczos: sym NB=%d NW=%d TPW=%d: %lld CTAs (%d per SM), %zu B smem/CTA\n", NB, NW, TPW,
+            grid, occ, dsm);
+  kern<<<(unsigned)grid, NW * 32, dsm, st>>>(M, src, out);
+  return cudaGetLastError();
+}
+
 template <int KM>
 size_t scratch_large() {
   return sizeof(float) * 2 * (size_t)KM * KM * (size_t)device_sms();
@@ -311,6 +338,17 @@ struct Variant {
     "cluster KB=" #KB " CS=" #CS " NTC=" #NTC " RPT=" #RPT,                                     \
         {launch_cluster<KB, CS, NTC, RPT>, nullptr}, {scratch_none, scratch_none}               \
   }
+// upper 32 x 32 tiles of A_S and P, one set per CTA (NB blocks of 32, NW warps of TPW tiles)
+#define SYM(NB, NW, TPW, MINB)                                                                 \
+  Variant {                                                                                      \
+    "sym NB=" #NB " NW=" #NW " TPW=" #TPW " MINB=" #MINB,                                        \
+        {launch_sym<NB, NW, TPW, MINB>, nullptr}, {scratch_none, scratch_none}                   \
+  }
+#define SYMR(NB, NW, TPW, REGS)                                                                \
+  Variant {                                                                                      \
+    "sym NB=" #NB " NW=" #NW " TPW=" #TPW " REGS=" #REGS,                                        \
+        {launch_sym<NB, NW, TPW, -(REGS)>, nullptr}, {scratch_none, scratch_none}                \
+  }
 #define LARGE(KM) \
   Variant {                                                                             \
     "large KM=" #KM " CTA=256", {launch_large<KM, false>, launch_large<KM, true>},      \
@@ -326,12 +364,14 @@ const std::vector<Variant>& variants(int b) {
       {REG(16, 2, 1, 128, 4), REG(16, 1, 1, 128, 4), SA(16, 2, 128, 4)},
       {REG(32, 2, 1, 128, 3), REG(32, 1, 1, 128, 4), SA(32, 2, 128, 4)},
       {REG(64, 1, 1, 128, 3), SA(64, 2, 128, 3), REG(64, 1, 1, 128, 2), SA(64, 2, 128, 2),
-       SAR(64, 2, 96, 224), SAR(64, 2, 128, 224), SAR(64, 2, 64, 200)},
-      {SA(128, 1, 128, 3), REG(128, 1, 2, 256, 1), SA(128, 1, 128, 2), SA2(128, 128, 2)},
+       SAR(64, 2, 96, 224), SAR(64, 2, 128, 224), SAR(64, 2, 64, 200), SYM(2, 3, 1, 6), SYM(2, 2, 2, 8)},
+      {SA(128, 1, 128, 3), REG(128, 1, 2, 256, 1), SA(128, 1, 128, 2), SA2(128, 128, 2), SYM(4, 5, 2, 3),
+       SYM(4, 5, 2, 4), SYM(4, 10, 1, 2), SYMR(4, 5, 2, 136)},
       {CLUSTER(192, 2, 384), LARGE(256), CLUSTER(192, 4, 192), CLUSTER(192, 1, 384), CLUSTER(192, 1, 768),
-       CLUSTERR(192, 1, 384, 2), CLUSTERR(192, 1, 384, 4)},
+       CLUSTERR(192, 1, 384, 2), CLUSTERR(192, 1, 384, 4), SYM(6, 7, 3, 2), SYM(6, 11, 2, 1), SYM(6, 21, 1, 1),
+       SYMR(6, 7, 3, 144)},
       {CLUSTER(256, 2, 512), LARGE(256), CLUSTER(256, 4, 256), CLUSTER(256, 8, 256), CLUSTER(256, 2, 256),
-       CLUSTERR(256, 2, 256, 2), CLUSTERR(256, 2, 256, 4)},
+       CLUSTERR(256, 2, 256, 2), CLUSTERR(256, 2, 256, 4), SYM(8, 12, 3, 1), SYM(8, 18, 2, 1)},
       {CLUSTER(384, 4, 384), LARGE(512), CLUSTER(384, 8, 192), CLUSTER(384, 6, 256), CLUSTERR(384, 6, 256, 2),
        CLUSTERR(384, 6, 256, 4), CLUSTERR(384, 4, 384, 4)},
       {CLUSTER(512, 8, 256), LARGE(512), CLUSTER(512, 8, 512), CLUSTERR(512, 8, 256, 2),
@@ -342,8 +382,8 @@ const std::vector<Variant>& variants(int b) {
 
 // Built-in shape per bin: the autotuner's choices on B200 (tuning.json), so a
 // caller that never runs the Python tuner (a C program, MATLAB) gets them too.
-const int kDefaultVariant[kNumBins] = {0, 0, 2, 5, 3, 6, 6, 6, 3};
-int g_variant[kNumBins] = {0, 0, 2, 5, 3, 6, 6, 6, 3};
+const int kDefaultVariant[kNumBins] = {0, 0, 2, 5, 3, 6, 7, 6, 3};
+int g_variant[kNumBins] = {0, 0, 2, 5, 3, 6, 7, 6, 3};
 
 int bin_of_k(int k) {
   for (int b = 0; b < kNumBins; ++b)

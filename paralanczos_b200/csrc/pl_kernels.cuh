@@ -6,6 +6,7 @@
 #include "pl_engine.cuh"
 #include "pl_engine_sa.cuh"
 #include "pl_engine_sa2.cuh"
+#include "pl_engine_sym.cuh"
 #include "pl_indexgen.cuh"
 #include "pl_queue.cuh"
 
@@ -264,6 +265,50 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(NTC, 1)
     }
     cluster_solve_set<KB, CS, NTC, RPT>(M, src.idx + off, k, set, out, sm, cl, rank);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Symmetric-tile form (pl_engine_sym.cuh): persistent, one set per CTA at a
+// time, A_S and P as upper 32 x 32 tiles (warp w holds tiles w, w + NW, ...).
+// ---------------------------------------------------------------------------
+template <int NB, int NW, int TPW>
+__device__ __forceinline__ void sym_kernel_body(const MatrixF32& M, const SetSource& src, const SetOutputs& out) {
+  static_assert(NW * TPW >= NB * (NB + 1) / 2, "every tile needs a warp");
+  static_assert(NW >= NB && NW <= 32, "one warp per row block, partials summed by one warp");
+  extern __shared__ __align__(16) float dsm[];
+  SymSmem<NB, NW>& sm = *reinterpret_cast<SymSmem<NB, NW>*>(dsm);
+  const int w = threadIdx.x >> 5;
+  int TI[TPW], TJ[TPW], TT[TPW];
+#pragma unroll
+  for (int u = 0; u < TPW; ++u) {
+    TT[u] = w + NW * u;
+    sym_tile<NB>(TT[u], TI[u], TJ[u]);
+  }
+  const long long nitems = item_count(src);
+  const int pbase = src.perm_start ? *src.perm_start : 0;
+  for (long long it = blockIdx.x; it < nitems; it += gridDim.x) {
+    long long set, off;
+    int k;
+    set_span(src, it, pbase, set, off, k);
+    if (k < 1 || k > 32 * NB) {
+      if (threadIdx.x == 0) write_failed(out, set, off, 0, SET_BAD_K);
+      continue;
+    }
+    sym_solve_set<NB, NW, TPW>(M, src.idx + off, k, set, out, sm, TI, TJ, TT);
+  }
+}
+
+template <int NB, int NW, int TPW, int MINB>
+__global__ void __launch_bounds__(NW * 32, MINB) k_sym_solve(MatrixF32 M, SetSource src, SetOutputs out) {
+  sym_kernel_body<NB, NW, TPW>(M, src, out);
+}
+
+// The same with an explicit register cap (the launch-bounds cap rounds the
+// block up to whole groups of 4 warps: 7 warps at 2 CTAs per SM would get 128
+// registers, where 144 fit).
+template <int NB, int NW, int TPW, int REGS>
+__global__ void __maxnreg__(REGS) k_sym_solve_r(MatrixF32 M, SetSource src, SetOutputs out) {
+  sym_kernel_body<NB, NW, TPW>(M, src, out);
 }
 
 // ---------------------------------------------------------------------------

@@ -1,6 +1,8 @@
 """Every thread-block-cluster shape of the large-k bins (one or several rows
-per thread, one or several CTAs per set), forced as its bin's kernel, in the
-extremes mode: random Gram subsets, zero-padded k, and breakdown restarts
+per thread, one or several CTAs per set) and every symmetric-tile shape (A_S
+and P as upper 32 x 32 tiles, one set per CTA), forced as its bin's kernel,
+in the extremes mode: random Gram subsets, zero-padded k (including sets
+that leave whole tile blocks empty), and breakdown restarts
 (a block-diagonal matrix whose all-ones start vector spans an invariant
 subspace), against FP64 LAPACK dsyev / numpy eigvalsh within 1e-5 relative.
 """
@@ -26,10 +28,11 @@ def _cluster_variants():
 def _list_cluster_variants():
     out = []
     for b in range(api.num_bins()):
-        if api.bin_kmax(b) <= 128:
-            continue
         nvar, _ = api.tune_describe(b, 0)
-        out += [(b, v) for v in range(nvar) if api.tune_describe(b, v)[1].startswith("cluster")]
+        for v in range(nvar):
+            d = api.tune_describe(b, v)[1]
+            if d.startswith("sym") or (d.startswith("cluster") and api.bin_kmax(b) > 128):
+                out.append((b, v))
     return out
 
 
@@ -51,7 +54,7 @@ def test_cluster_shape(bv):
     rng = np.random.default_rng(100 + b * 10 + v)
     Phi = rng.standard_normal((1024, 2048)) / np.sqrt(1024)
     A = (Phi.T @ Phi).astype(np.float32)
-    for k in (kmax, kmax - 13):
+    for k in (kmax, kmax - 13, kmax - 40):
         _, idx = O.gen_stream(200 + k, 0, 6, 2048, 0, k, k)
         res = _solve(A, idx, k, b, v)
         assert ((res["err"] & ~_lib.PL_SET_BREAKDOWN) == 0).all()
