@@ -265,15 +265,10 @@ cudaError_t launch_cluster(const MatrixF32& M, const SetSource& src, const SetOu
   return cudaGetLastError();
 }
 
-// MINB > 0: launch-bounds form; MINB < 0: register cap of -MINB (k_sym_solve_r)
 template <int NB, int NW, int TPW, int MINB>
 cudaError_t launch_sym(const MatrixF32& M, const SetSource& src, const SetOutputs& out, long long nitems,
                        void*, cudaStream_t st, bool prep) {
-  void (*kern)(MatrixF32, SetSource, SetOutputs);
-  if constexpr (MINB > 0)
-    kern = k_sym_solve<NB, NW, TPW, MINB>;
-  else
-    kern = k_sym_solve_r<NB, NW, TPW, -MINB>;
+  auto kern = k_sym_solve<NB, NW, TPW, MINB>;
   const size_t dsm = sizeof(SymSmem<NB, NW>);
   static int occ = [&] {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
@@ -344,11 +339,6 @@ struct Variant {
     "sym NB=" #NB " NW=" #NW " TPW=" #TPW " MINB=" #MINB,                                        \
         {launch_sym<NB, NW, TPW, MINB>, nullptr}, {scratch_none, scratch_none}                   \
   }
-#define SYMR(NB, NW, TPW, REGS)                                                                \
-  Variant {                                                                                      \
-    "sym NB=" #NB " NW=" #NW " TPW=" #TPW " REGS=" #REGS,                                        \
-        {launch_sym<NB, NW, TPW, -(REGS)>, nullptr}, {scratch_none, scratch_none}                \
-  }
 #define LARGE(KM) \
   Variant {                                                                             \
     "large KM=" #KM " CTA=256", {launch_large<KM, false>, launch_large<KM, true>},      \
@@ -364,14 +354,14 @@ const std::vector<Variant>& variants(int b) {
       {REG(16, 2, 1, 128, 4), REG(16, 1, 1, 128, 4), SA(16, 2, 128, 4)},
       {REG(32, 2, 1, 128, 3), REG(32, 1, 1, 128, 4), SA(32, 2, 128, 4)},
       {REG(64, 1, 1, 128, 3), SA(64, 2, 128, 3), REG(64, 1, 1, 128, 2), SA(64, 2, 128, 2),
-       SAR(64, 2, 96, 224), SAR(64, 2, 128, 224), SAR(64, 2, 64, 200), SYM(2, 3, 1, 6), SYM(2, 2, 2, 8)},
+       SAR(64, 2, 96, 224), SAR(64, 2, 128, 224), SAR(64, 2, 64, 200)},
       {SA(128, 1, 128, 3), REG(128, 1, 2, 256, 1), SA(128, 1, 128, 2), SA2(128, 128, 2), SYM(4, 5, 2, 3),
-       SYM(4, 5, 2, 4), SYM(4, 10, 1, 2), SYMR(4, 5, 2, 136)},
+       SYM(4, 10, 1, 2)},
       {CLUSTER(192, 2, 384), LARGE(256), CLUSTER(192, 4, 192), CLUSTER(192, 1, 384), CLUSTER(192, 1, 768),
-       CLUSTERR(192, 1, 384, 2), CLUSTERR(192, 1, 384, 4), SYM(6, 7, 3, 2), SYM(6, 11, 2, 1), SYM(6, 21, 1, 1),
-       SYMR(6, 7, 3, 144)},
+       CLUSTERR(192, 1, 384, 2), CLUSTERR(192, 1, 384, 4), SYM(6, 11, 2, 1), SYM(6, 21, 1, 1),
+       SYM(6, 16, 2, 1)},
       {CLUSTER(256, 2, 512), LARGE(256), CLUSTER(256, 4, 256), CLUSTER(256, 8, 256), CLUSTER(256, 2, 256),
-       CLUSTERR(256, 2, 256, 2), CLUSTERR(256, 2, 256, 4), SYM(8, 12, 3, 1), SYM(8, 18, 2, 1)},
+       CLUSTERR(256, 2, 256, 2), CLUSTERR(256, 2, 256, 4), SYM(8, 12, 3, 1)},
       {CLUSTER(384, 4, 384), LARGE(512), CLUSTER(384, 8, 192), CLUSTER(384, 6, 256), CLUSTERR(384, 6, 256, 2),
        CLUSTERR(384, 6, 256, 4), CLUSTERR(384, 4, 384, 4)},
       {CLUSTER(512, 8, 256), LARGE(512), CLUSTER(512, 8, 512), CLUSTERR(512, 8, 256, 2),

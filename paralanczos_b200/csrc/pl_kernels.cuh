@@ -303,14 +303,6 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_sym_solve(MatrixF32 M, SetSou
   sym_kernel_body<NB, NW, TPW>(M, src, out);
 }
 
-// The same with an explicit register cap (the launch-bounds cap rounds the
-// block up to whole groups of 4 warps: 7 warps at 2 CTAs per SM would get 128
-// registers, where 144 fit).
-template <int NB, int NW, int TPW, int REGS>
-__global__ void __maxnreg__(REGS) k_sym_solve_r(MatrixF32 M, SetSource src, SetOutputs out) {
-  sym_kernel_body<NB, NW, TPW>(M, src, out);
-}
-
 // ---------------------------------------------------------------------------
 // Binning of a CSR set list by k (device-side counting sort of set ids).
 // ---------------------------------------------------------------------------
