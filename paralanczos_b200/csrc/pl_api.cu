@@ -166,6 +166,38 @@ size_t scratch_sar() {
   return grid * (CTA / NT) * (NT / 2) * KB * sizeof(double2);
 }
 
+// shared-A with the next set's triangle prefetched (extremes mode)
+template <int KB, int RPT, int CTA, int REGS>
+cudaError_t launch_sap(const MatrixF32& M, const SetSource& src, const SetOutputs& out, long long nitems,
+                       void* scratch, cudaStream_t st, bool prep) {
+  auto kern = k_sa_solve_p<KB, RPT, CTA, REGS>;
+  constexpr int GPC = CTA / CfgSA<KB, RPT>::NT;
+  const size_t dsm = (sizeof(SASmem<KB, RPT>) + sizeof(SAStage<KB, CfgSA<KB, RPT>::NT>)) * GPC;
+  static int occ = [&] {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
+    cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    return occupancy(kern, CTA, dsm);
+  }();
+  if (prep) {
+    cudaFuncAttributes fa;
+    return cudaFuncGetAttributes(&fa, kern);
+  }
+  const long long grid = grid_for(nitems, GPC, occ);
+  kern<<<(unsigned)grid, CTA, dsm, st>>>(M, src, out, (double2*)scratch);
+  return cudaGetLastError();
+}
+
+template <int KB, int RPT, int CTA, int REGS>
+size_t scratch_sap() {
+  auto kern = k_sa_solve_p<KB, RPT, CTA, REGS>;
+  constexpr int NT = CfgSA<KB, RPT>::NT;
+  const size_t dsm = (sizeof(SASmem<KB, RPT>) + sizeof(SAStage<KB, CfgSA<KB, RPT>::NT>)) * (CTA / NT);
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
+  cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  const size_t grid = (size_t)device_sms() * occupancy(kern, CTA, dsm);
+  return grid * (CTA / NT) * (NT / 2) * KB * sizeof(double2);
+}
+
 template <int KB, int CTA, int MINB>
 cudaError_t launch_sa2(const MatrixF32& M, const SetSource& src, const SetOutputs& out,
                        long long nitems, void* scratch, cudaStream_t st, bool prep) {
@@ -317,6 +349,12 @@ struct Variant {
         {launch_sar<KB, RPT, CTA, REGS, false>, launch_sar<KB, RPT, CTA, REGS, true>},        \
         {scratch_sar<KB, RPT, CTA, REGS, false>, scratch_none}                                 \
   }
+// the next set's upper triangle prefetched into shared memory during this set's steps
+#define SAP(KB, RPT, CTA, REGS)                                                              \
+  Variant {                                                                                    \
+    "sharedA prefetch KB=" #KB " RPT=" #RPT " CTA=" #CTA " REGS=" #REGS,                       \
+        {launch_sap<KB, RPT, CTA, REGS>, nullptr}, {scratch_sap<KB, RPT, CTA, REGS>, scratch_none} \
+  }
 #define SA2(KB, CTA, MINB)                                                                   \
   Variant {                                                                                    \
     "sharedA 2 threads/row KB=" #KB " CTA=" #CTA " MINB=" #MINB,                               \
@@ -352,9 +390,10 @@ const std::vector<Variant>& variants(int b) {
   static const std::vector<Variant> v[kNumBins] = {
       {REG(8, 2, 1, 128, 4), REG(8, 1, 1, 128, 4), SA(8, 2, 128, 4)},
       {REG(16, 2, 1, 128, 4), REG(16, 1, 1, 128, 4), SA(16, 2, 128, 4)},
-      {REG(32, 2, 1, 128, 3), REG(32, 1, 1, 128, 4), SA(32, 2, 128, 4)},
+      {REG(32, 2, 1, 128, 3), REG(32, 1, 1, 128, 4), SA(32, 2, 128, 4), SAP(32, 2, 128, 128)},
       {REG(64, 1, 1, 128, 3), SA(64, 2, 128, 3), REG(64, 1, 1, 128, 2), SA(64, 2, 128, 2),
-       SAR(64, 2, 96, 224), SAR(64, 2, 128, 224), SAR(64, 2, 64, 200)},
+       SAR(64, 2, 96, 224), SAR(64, 2, 128, 224), SAR(64, 2, 64, 200), SAP(64, 2, 128, 224),
+       SAP(64, 2, 64, 224), SAP(64, 2, 96, 224)},
       {SA(128, 1, 128, 3), REG(128, 1, 2, 256, 1), SA(128, 1, 128, 2), SA2(128, 128, 2), SYM(4, 5, 2, 3),
        SYM(4, 10, 1, 2)},
       {CLUSTER(192, 2, 384), LARGE(256), CLUSTER(192, 4, 192), CLUSTER(192, 1, 384), CLUSTER(192, 1, 768),
@@ -372,8 +411,8 @@ const std::vector<Variant>& variants(int b) {
 
 // Built-in shape per bin: the autotuner's choices on B200 (tuning.json), so a
 // caller that never runs the Python tuner (a C program, MATLAB) gets them too.
-const int kDefaultVariant[kNumBins] = {0, 0, 2, 5, 3, 6, 7, 6, 3};
-int g_variant[kNumBins] = {0, 0, 2, 5, 3, 6, 7, 6, 3};
+const int kDefaultVariant[kNumBins] = {0, 0, 2, 7, 3, 6, 7, 6, 3};
+int g_variant[kNumBins] = {0, 0, 2, 7, 3, 6, 7, 6, 3};
 
 int bin_of_k(int k) {
   for (int b = 0; b < kNumBins; ++b)

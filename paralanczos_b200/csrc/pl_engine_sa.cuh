@@ -44,24 +44,120 @@ __device__ __forceinline__ int sa_at(int r, int c) {
   return (((r / NT) * NCH + (c >> 2)) * NT + (r % NT)) * 4 + (c & 3);
 }
 
-template <int KB, int RPT, bool ALL>
+// Prefetch of the next set's upper triangle (the PF variants).  While a group
+// runs its set's Lanczos steps, its threads issue cp.async copies of the next
+// set's k(k+1)/2 random elements of A into a shared-memory stage, a few per
+// step; they need no registers and land long before the set ends.  The next
+// set then mirrors the stage into its A_S layout instead of gathering from
+// global memory.  Thread t stages exactly the elements it would have
+// gathered, at e[ii * NT + t] (its ii-th), so it reads back only its own
+// copies.
+struct SANext {
+  SetMatrix SM;
+  const int* S;
+  int k;
+  bool valid;
+};
+
+template <int KB, int NT>
+struct __align__(16) SAStage {
+  static constexpr int NP = KB / 2, TPP = NT / NP, PER = (KB + TPP) / TPP;
+  float e[PER * NT];
+  int idx[KB];  // the next set's indices, -1 outside [0, n)
+};
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// The issuing side of the prefetch for one thread: the triangle order of the
+// gather (rows p and KB-1-p paired, TPP threads per pair), PKS elements per
+// Lanczos step.
+template <int KB, int NT>
+struct TriPrefetch {
+  static constexpr int NP = KB / 2, TPP = NT / NP, PER = (KB + TPP) / TPP;
+  static constexpr int PKS = (PER + 31) / 32;
+  static_assert(NP * TPP == NT, "row pairs per group");
+  const float* row0 = nullptr;
+  const float* row1 = nullptr;
+  int k = 0, pf = 0;
+  bool on = false;
+
+  // the next set's indices into stg->idx (checked), its two row pointers
+  template <class G>
+  __device__ __forceinline__ void setup(const SANext* nx, SAStage<KB, NT>* stg, const G& g) {
+    const int t = g.t, p = t % NP;
+    g.sync();  // the previous prefetch's readers of stg->idx are done
+    for (int c = t; c < KB; c += NT) {
+      int v = -1;
+      if (c < nx->k) {
+        v = nx->SM.index(nx->S, c);
+        if (v < 0 || v >= nx->SM.n) v = -1;
+      }
+      stg->idx[c] = v;
+    }
+    g.sync();
+    const int a0 = stg->idx[p], a1 = stg->idx[KB - 1 - p];
+    row0 = a0 >= 0 ? nx->SM.A + (size_t)a0 * (size_t)nx->SM.lda : nullptr;
+    row1 = a1 >= 0 ? nx->SM.A + (size_t)a1 * (size_t)nx->SM.lda : nullptr;
+    k = nx->k;
+    pf = 0;
+    on = true;
+  }
+  __device__ __forceinline__ void issue(SAStage<KB, NT>* stg, int t, int ii) const {
+    const int p = t % NP, i = (t / NP) * PER + ii;
+    if (TPP > 1 && i > KB) return;
+    const bool first = i < KB - p;
+    const int r = first ? p : KB - 1 - p;
+    const int c = first ? p + i : i - 1;
+    if (r < k && c < k) {
+      const int ci = stg->idx[c];
+      const float* row = first ? row0 : row1;
+      if (row && ci >= 0) cp_async4(&stg->e[ii * NT + t], row + ci);
+    }
+  }
+  __device__ __forceinline__ void step(SAStage<KB, NT>* stg, int t) {
+    if (on)
+      for (int q = 0; q < PKS && pf < PER; ++q, ++pf) issue(stg, t, pf);
+  }
+  __device__ __forceinline__ void finish(SAStage<KB, NT>* stg, int t) {
+    if (on)
+      for (; pf < PER; ++pf) issue(stg, t, pf);
+  }
+};
+
+template <int KB, int RPT, bool ALL, bool PF = false>
 __device__ __forceinline__ int solve_set_sa(const MatrixF32& M, const int* __restrict__ S, int k,
                                              long long set, long long off, const SetOutputs& out,
                                              SASmem<KB, RPT>& sm,
-                                             const Grp<CfgSA<KB, RPT>::NT>& g) {
+                                             const Grp<CfgSA<KB, RPT>::NT>& g,
+                                             SAStage<KB, KB / RPT>* stg = nullptr, bool have = false,
+                                             const SANext* nx = nullptr, bool* issued = nullptr) {
   using C = CfgSA<KB, RPT>;
   constexpr int NT = C::NT;
   constexpr int NW = C::NW;
   constexpr int NCH = C::NCH;
   const int t = g.t;
+  if constexpr (PF) {
+    static_assert(RPT <= 2 && !ALL, "the prefetch follows the triangle gather (extremes mode)");
+    *issued = false;
+    if (have) cp_async_wait_all();  // this set's stage (issued a whole set ago)
+  }
 
   // ---- indices -> shared memory, validation ---------------------------------
+  // (a prefetched set's indices were read and checked by the previous set:
+  // stg->idx, -1 where outside [0, n))
   const SetMatrix SM = set_matrix(M, set);
   bool bad = false;
   for (int c = t; c < KB; c += NT) {
     int v = 0;
     if (c < k) {
-      v = SM.index(S, c);
+      if (PF && have)
+        v = stg->idx[c];
+      else
+        v = SM.index(S, c);
       bad |= (v < 0) | (v >= SM.n);
     }
     sm.idx[c] = (c < k && v >= 0 && v < SM.n) ? v : 0;
@@ -104,7 +200,13 @@ __device__ __forceinline__ int solve_set_sa(const MatrixF32& M, const int* __res
         const bool first = i < KB - p;
         const int r = first ? r0 : r1;
         const int c = first ? p + i : i - 1;  // c >= r
-        const float e = (r < k && c < k) ? __ldg((first ? row0 : row1) + sm.idx[c]) : 0.f;
+        float e = 0.f;
+        if (r < k && c < k) {
+          if (PF && have)
+            e = stg->e[ii * NT + t];
+          else
+            e = __ldg((first ? row0 : row1) + sm.idx[c]);
+        }
         const double e2 = (double)e * (double)e;
         fro += (c == r) ? e2 : 2.0 * e2;
         Af[sa_at<NT, NCH>(r, c)] = e;
@@ -160,6 +262,12 @@ __device__ __forceinline__ int solve_set_sa(const MatrixF32& M, const int* __res
   const double fro2 = group_sum<NT, NW>(fro, g, sm.red[2]);
   const double tau = 32.0 * (double)kEps32 * sqrt(fro2);
 
+  // ---- the next set's prefetch: its indices, then its elements over the steps -
+  TriPrefetch<KB, PF ? NT : KB> pre;  // (a valid shape when unused)
+  if constexpr (PF) {
+    if (nx->valid) pre.setup(nx, stg, g);
+  }
+
   // ---- Lanczos with projector reorthogonalisation ----------------------------
   float v[RPT], vp[RPT];
   const float v0 = (float)(1.0 / sqrt((double)k));
@@ -175,6 +283,7 @@ __device__ __forceinline__ int solve_set_sa(const MatrixF32& M, const int* __res
   g.sync();
 
   for (int j = 0; j < k; ++j) {
+    if constexpr (PF) pre.step(stg, t);
     // P -= v v^T and y = A v, one pass over the broadcast vector
     float2 ya[RPT], yb[RPT], ncoef[RPT];
 #pragma unroll
@@ -311,6 +420,10 @@ __device__ __forceinline__ int solve_set_sa(const MatrixF32& M, const int* __res
     }
   }
   g.sync();  // T visible to every thread
+  if constexpr (PF) {
+    pre.finish(stg, t);  // what the steps left (small k, early exit)
+    *issued = pre.on;
+  }
 
   if constexpr (!ALL) {
     // extremes mode: T stays in sm.ab for the caller's deferred bisection

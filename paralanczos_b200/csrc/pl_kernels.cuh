@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(CTA, MINB)
 // Batched form, shared-A engine (pl_engine_sa.cuh): persistent, A_S in
 // dynamic shared memory, P in registers.
 // ---------------------------------------------------------------------------
-template <int KB, int RPT, int CTA, bool ALL>
+template <int KB, int RPT, int CTA, bool ALL, bool PF = false>
 __device__ __forceinline__ void sa_solve_body(const MatrixF32& M, const SetSource& src, const SetOutputs& out,
                                               double2* __restrict__ qbuf) {
   using C = CfgSA<KB, RPT>;
@@ -88,6 +88,10 @@ __device__ __forceinline__ void sa_solve_body(const MatrixF32& M, const SetSourc
   const long long nitems = item_count(src);
   const int pbase = src.perm_start ? *src.perm_start : 0;
   double2* __restrict__ T = qbuf + ((size_t)blockIdx.x * GPC + gic) * (size_t)(Q * KB);
+  // PF: the next set's triangle is staged behind this set's steps (SAStage
+  // after the GPC SASmem slots)
+  SAStage<KB, C::NT>* stg = PF ? reinterpret_cast<SAStage<KB, C::NT>*>(smem + GPC) + gic : nullptr;
+  bool have = false;  // stg holds this set's elements
   int nq = 0;
   for (long long it = (long long)blockIdx.x * GPC + gic; it < nitems; it += ng) {
     long long set, off;
@@ -95,14 +99,30 @@ __device__ __forceinline__ void sa_solve_body(const MatrixF32& M, const SetSourc
     set_span(src, it, pbase, set, off, k);
     if (k < 1 || k > KB) {
       if (g.t == 0) write_failed(out, set, off, 0, SET_BAD_K);
+      have = false;
       continue;
+    }
+    SANext nx{};
+    nx.valid = false;
+    if constexpr (PF) {
+      const long long itn = it + ng;
+      if (itn < nitems) {
+        long long setn, offn;
+        int kn;
+        set_span(src, itn, pbase, setn, offn, kn);
+        const SetMatrix SMn = set_matrix(M, setn);
+        if (kn >= 1 && kn <= KB && !SMn.local) nx = SANext{SMn, src.idx + offn, kn, true};
+      }
     }
     // the slot's metadata goes to shared memory first, so the set id and k
     // need no registers across the Lanczos loop
     if constexpr (!ALL) {
       if (g.t == 0) qmeta[gic][nq] = QueueMeta{set, k, 0};
     }
-    const int st = solve_set_sa<KB, RPT, ALL>(M, src.idx + off, k, set, off, out, smem[gic], g);
+    bool issued = false;
+    const int st = solve_set_sa<KB, RPT, ALL, PF>(M, src.idx + off, k, set, off, out, smem[gic], g, stg, have,
+                                                  &nx, &issued);
+    have = issued;
     if constexpr (!ALL) {
       if (st >= 0) {
         const int kq = qmeta[gic][nq].k;
@@ -121,6 +141,7 @@ __device__ __forceinline__ void sa_solve_body(const MatrixF32& M, const SetSourc
   if constexpr (!ALL) {
     if (nq > 0) queue_bisect(T, Q, nq, qmeta[gic], g.t, out, g.mask);
   }
+  if constexpr (PF) cp_async_wait_all();  // no copy outlives the kernel
 }
 
 template <int KB, int RPT, int CTA, int MINB, bool ALL>
@@ -135,6 +156,14 @@ template <int KB, int RPT, int CTA, int REGS, bool ALL>
 __global__ void __maxnreg__(REGS) k_sa_solve_r(MatrixF32 M, SetSource src, SetOutputs out,
                                                double2* __restrict__ qbuf) {
   sa_solve_body<KB, RPT, CTA, ALL>(M, src, out, qbuf);
+}
+
+// The same with the next set's triangle prefetched into a shared-memory stage
+// (extremes mode).
+template <int KB, int RPT, int CTA, int REGS>
+__global__ void __maxnreg__(REGS) k_sa_solve_p(MatrixF32 M, SetSource src, SetOutputs out,
+                                               double2* __restrict__ qbuf) {
+  sa_solve_body<KB, RPT, CTA, false, true>(M, src, out, qbuf);
 }
 
 // ---------------------------------------------------------------------------
