@@ -234,7 +234,7 @@ def run_c3(args):
                      "e2e": {"value": nsets / e2e_s, "unit": "solves/s",
                              "h2d_bytes_per_step": int(A_h.numel() * 4 + idx_p.numel() * 4 + off_p.numel() * 8),
                              "d2h_bytes_per_step": int(nsets * 28), "path": "pl_solve_host, CSR offsets"},
-                     "gpu_launches": args.steps * 13,
+                     "gpu_launches": args.steps * (4 + api.num_bins()),
                      "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                                   "frac": achieved / peak, "traffic": None,
                                   "algorithmic": "sum over sets of 4k^3 FLOP"},

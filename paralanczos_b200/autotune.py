@@ -98,11 +98,26 @@ def apply(path: str | None = None, lib=None) -> bool:
             return False
     except Exception:
         return False
+    import ctypes
+
     from . import _lib
     L = lib or _lib.lib()
-    for b, ent in data.get("bins", {}).items():
-        if L.pl_tune_set(int(b), int(ent["variant"])) != 0:
-            return False
+    # entries are matched by the bin's k range and the variant's description,
+    # so a file written by a build with other bins or variants still applies
+    # to what it names (the rest keep their built-in defaults)
+    bin_of = {L.pl_bin_kmax(b): b for b in range(L.pl_num_bins())}
+    buf = ctypes.create_string_buffer(256)
+    for ent in data.get("bins", {}).values():
+        b = bin_of.get(int(ent.get("kmax", -1)))
+        if b is None:
+            continue
+        nvar = L.pl_tune_describe(b, 0, buf, 256)
+        for v in range(nvar):
+            L.pl_tune_describe(b, v, buf, 256)
+            if buf.value.decode() == ent.get("desc"):
+                if L.pl_tune_set(b, v) != 0:
+                    return False
+                break
     return True
 
 

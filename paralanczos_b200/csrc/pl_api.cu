@@ -383,8 +383,8 @@ struct Variant {
         {scratch_large<KM>, scratch_large<KM>}                                           \
   }
 
-const int kBinK[] = {8, 16, 32, 64, 128, 192, 256, 384, 512};
-constexpr int kNumBins = 9;
+const int kBinK[] = {8, 16, 32, 64, 96, 128, 192, 256, 384, 512};
+constexpr int kNumBins = 10;
 
 const std::vector<Variant>& variants(int b) {
   static const std::vector<Variant> v[kNumBins] = {
@@ -394,6 +394,7 @@ const std::vector<Variant>& variants(int b) {
       {REG(64, 1, 1, 128, 3), SA(64, 2, 128, 3), REG(64, 1, 1, 128, 2), SA(64, 2, 128, 2),
        SAR(64, 2, 96, 224), SAR(64, 2, 128, 224), SAR(64, 2, 64, 200), SAP(64, 2, 128, 224),
        SAP(64, 2, 64, 224), SAP(64, 2, 96, 224)},
+      {SA(96, 1, 96, 3), SA2(96, 96, 3), SA2(96, 96, 4), SA(96, 1, 96, 4)},
       {SA(128, 1, 128, 3), REG(128, 1, 2, 256, 1), SA(128, 1, 128, 2), SA2(128, 128, 2), SYM(4, 5, 2, 3),
        SYM(4, 10, 1, 2)},
       {CLUSTER(192, 2, 384), LARGE(256), CLUSTER(192, 4, 192), CLUSTER(192, 1, 384), CLUSTER(192, 1, 768),
@@ -411,8 +412,8 @@ const std::vector<Variant>& variants(int b) {
 
 // Built-in shape per bin: the autotuner's choices on B200 (tuning.json), so a
 // caller that never runs the Python tuner (a C program, MATLAB) gets them too.
-const int kDefaultVariant[kNumBins] = {0, 0, 2, 7, 3, 6, 7, 6, 3};
-int g_variant[kNumBins] = {0, 0, 2, 7, 3, 6, 7, 6, 3};
+const int kDefaultVariant[kNumBins] = {0, 0, 2, 7, 1, 3, 6, 7, 6, 3};
+int g_variant[kNumBins] = {0, 0, 2, 7, 1, 3, 6, 7, 6, 3};
 
 int bin_of_k(int k) {
   for (int b = 0; b < kNumBins; ++b)
@@ -632,11 +633,11 @@ int solve_csr(const MatrixF32& M, const int* idx, const long long* offsets, long
   rc = ensure(d.large, qtotal > 0 ? qtotal : 256);
   if (rc) return rc;
   char keybuf[512];
-  snprintf(keybuf, sizeof keybuf, "%p|%d|%lld|%p|%p|%lld|%d|%p|%p|%p|%p|%p|%p|%d%d%d%d%d%d%d",
-           (const void*)M.A, M.n, M.lda, (const void*)idx, (const void*)offsets, nsets, form,
-           (void*)out.lmin, (void*)out.lmax, (void*)out.delta, (void*)out.err, (void*)out.eig,
-           (void*)out.det, g_variant[0], g_variant[1], g_variant[2], g_variant[3], g_variant[4],
-           g_variant[5], g_variant[6], g_variant[7] * 10 + g_variant[8]);
+  int kl = snprintf(keybuf, sizeof keybuf, "%p|%d|%lld|%p|%p|%lld|%d|%p|%p|%p|%p|%p|%p|", (const void*)M.A, M.n,
+                    M.lda, (const void*)idx, (const void*)offsets, nsets, form, (void*)out.lmin,
+                    (void*)out.lmax, (void*)out.delta, (void*)out.err, (void*)out.eig, (void*)out.det);
+  for (int b = 0; b < kNumBins && kl > 0 && kl < (int)sizeof keybuf - 4; ++b)
+    kl += snprintf(keybuf + kl, sizeof keybuf - (size_t)kl, "%d,", g_variant[b]);
   const std::string key(keybuf);
   auto it = d.graphs.find(key);
   if (it == d.graphs.end()) {

@@ -1,9 +1,11 @@
-"""The k <= 128 shared-A engine with two threads per row (k_sa2_solve), forced
-as the k <= 128 bin's kernel, against FP64 LAPACK dsyev: uniform k (full and
+"""The shared-A engine with two threads per row (k_sa2_solve), forced as the
+kernel of the 64 < k <= 96 and 96 < k <= 128 bins, against FP64 LAPACK dsyev: uniform k (full and
 zero-padded), uneven k with bad indices, breakdown restarts, NaN input, and
 pre-formed Gram blocks (its float4 path).  Extremes only: the all-eigenvalue
 mode of the bin uses the other shapes.
 """
+import contextlib
+
 import numpy as np
 import pytest
 
@@ -12,12 +14,29 @@ from paralanczos_b200 import _lib, api
 
 pytestmark = pytest.mark.gpu
 RTOL = 1e-5
-BIN = 4  # 64 < k <= 128
 
 
-def _variant():
-    nvar, _ = api.tune_describe(BIN, 0)
-    return next(v for v in range(nvar) if "2 threads/row" in api.tune_describe(BIN, v)[1])
+def _bins():
+    """The bins this engine serves: 64 < k <= 96 and 96 < k <= 128."""
+    return [b for b in range(api.num_bins()) if api.bin_kmax(b) in (96, 128)]
+
+
+def _variant(b):
+    nvar, _ = api.tune_describe(b, 0)
+    return next(v for v in range(nvar) if "2 threads/row" in api.tune_describe(b, v)[1])
+
+
+@contextlib.contextmanager
+def _forced():
+    bins = _bins()
+    assert len(bins) == 2
+    for b in bins:
+        api.tune_set(b, _variant(b))
+    try:
+        yield
+    finally:
+        for b in bins:
+            api.tune_set(b, -1)
 
 
 def _gram(M, N, seed):
@@ -28,13 +47,10 @@ def _gram(M, N, seed):
 
 def _run(A, idx, k=None, offsets=None):
     import torch
-    api.tune_set(BIN, _variant())
-    try:
+    with _forced():
         out = api.solve(torch.from_numpy(A).cuda(), torch.from_numpy(idx).cuda(), k=k,
                         offsets=None if offsets is None else torch.from_numpy(offsets).cuda())
         torch.cuda.synchronize()
-    finally:
-        api.tune_set(BIN, -1)
     return {n: t.cpu().numpy() for n, t in out.items()}
 
 
@@ -48,7 +64,7 @@ def _check(A, idx, res, k=None, offsets=None, skip=()):
         assert res["delta"][s] == max(1 - res["lmin"][s], res["lmax"][s] - 1)
 
 
-@pytest.mark.parametrize("k", [128, 97, 65])
+@pytest.mark.parametrize("k", [128, 97, 96, 65])
 def test_uniform_k_vs_dsyev(k):
     A = _gram(1024, 4096, 0)
     _, idx = O.gen_stream(60 + k, 0, 1200, 4096, 0, k, k)
@@ -75,7 +91,7 @@ def test_uneven_k_with_bad_indices():
     _check(A, idx, res, offsets=offsets, skip=set(bad))
 
 
-@pytest.mark.parametrize("k", [128, 100])
+@pytest.mark.parametrize("k", [128, 100, 96, 66])
 def test_breakdown_restart_extremes(k):
     for A in (np.eye(k, dtype=np.float32) * 2.0,
               np.kron(np.eye(2), np.ones((k // 2, k // 2))).astype(np.float32) + np.eye(k, dtype=np.float32)):
@@ -97,22 +113,21 @@ def test_nonfinite_input():
     assert ((res["err"][~has] & ~_lib.PL_SET_BREAKDOWN) == 0).all()
 
 
-def test_preformed_gram_blocks():
-    """The on-the-fly Gram form's shape (Phi 2048 x 4096, k = 128) solved on
-    its pre-formed blocks: within 1e-5 relative of dsyev on the FP64 Gram."""
+@pytest.mark.parametrize("k", [128, 96])
+def test_preformed_gram_blocks(k):
+    """The on-the-fly Gram form's shape (Phi 2048 x 4096, k = 128; and k = 96)
+    solved on its pre-formed blocks: within 1e-5 relative of dsyev on the FP64
+    Gram."""
     import torch
     rng = np.random.default_rng(9)
-    M, N, k = 2048, 4096, 128
+    M, N = 2048, 4096
     Phi = (rng.standard_normal((M, N)) / np.sqrt(M)).astype(np.float32)
     gf = api.GramFrame(torch.from_numpy(Phi).cuda())
     _, idx = O.gen_stream(73, 0, 200, N, 0, k, k)
     di = torch.from_numpy(idx).cuda()
-    api.tune_set(BIN, _variant())
-    try:
+    with _forced():
         out = gf.solve(di, k)
         torch.cuda.synchronize()
-    finally:
-        api.tune_set(BIN, -1)
     assert ((out["err"].cpu().numpy() & ~_lib.PL_SET_BREAKDOWN) == 0).all()
     lmin, lmax = out["lmin"].cpu().numpy(), out["lmax"].cpu().numpy()
     Phi64 = Phi.astype(np.float64)
