@@ -383,14 +383,15 @@ struct Variant {
         {scratch_large<KM>, scratch_large<KM>}                                           \
   }
 
-const int kBinK[] = {8, 16, 32, 64, 96, 128, 192, 256, 384, 512};
-constexpr int kNumBins = 10;
+const int kBinK[] = {8, 16, 32, 48, 64, 96, 128, 192, 256, 384, 512};
+constexpr int kNumBins = 11;
 
 const std::vector<Variant>& variants(int b) {
   static const std::vector<Variant> v[kNumBins] = {
       {REG(8, 2, 1, 128, 4), REG(8, 1, 1, 128, 4), SA(8, 2, 128, 4)},
       {REG(16, 2, 1, 128, 4), REG(16, 1, 1, 128, 4), SA(16, 2, 128, 4)},
       {REG(32, 2, 1, 128, 3), REG(32, 1, 1, 128, 4), SA(32, 2, 128, 4), SAP(32, 2, 128, 128)},
+      {SA(48, 3, 128, 2), REG(48, 3, 2, 128, 2)},
       {REG(64, 1, 1, 128, 3), SA(64, 2, 128, 3), REG(64, 1, 1, 128, 2), SA(64, 2, 128, 2),
        SAR(64, 2, 96, 224), SAR(64, 2, 128, 224), SAR(64, 2, 64, 200), SAP(64, 2, 128, 224),
        SAP(64, 2, 64, 224), SAP(64, 2, 96, 224)},
@@ -412,8 +413,8 @@ const std::vector<Variant>& variants(int b) {
 
 // Built-in shape per bin: the autotuner's choices on B200 (tuning.json), so a
 // caller that never runs the Python tuner (a C program, MATLAB) gets them too.
-const int kDefaultVariant[kNumBins] = {0, 0, 2, 7, 1, 3, 6, 7, 6, 3};
-int g_variant[kNumBins] = {0, 0, 2, 7, 1, 3, 6, 7, 6, 3};
+const int kDefaultVariant[kNumBins] = {0, 0, 2, 0, 7, 1, 3, 6, 7, 6, 3};
+int g_variant[kNumBins] = {0, 0, 2, 0, 7, 1, 3, 6, 7, 6, 3};
 
 int bin_of_k(int k) {
   for (int b = 0; b < kNumBins; ++b)

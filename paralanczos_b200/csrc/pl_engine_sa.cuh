@@ -61,7 +61,9 @@ struct SANext {
 
 template <int KB, int NT>
 struct __align__(16) SAStage {
-  static constexpr int NP = KB / 2, TPP = NT / NP, PER = (KB + TPP) / TPP;
+  // (groups of fewer than KB / 2 threads never prefetch; TPP = 1 keeps the
+  // type complete for them)
+  static constexpr int NP = KB / 2, TPP = NT >= NP ? NT / NP : 1, PER = (KB + TPP) / TPP;
   float e[PER * NT];
   int idx[KB];  // the next set's indices, -1 outside [0, n)
 };
