@@ -67,11 +67,12 @@ int pl_last_cuda_error(void);              /* cudaError_t of the last PL_ECUDA *
 
 /*
  * Solve every set (device pointers).
- *   A       n x n symmetric FP32 matrix, row-major, leading dimension lda >= n
- *           (the batched kernels that keep A[S,S] in shared memory, the tuned
- *           choice for 32 < k <= 192, read one triangle of it: for positions
- *           r <= c of a set only A[S[r]][S[c]], so an A that is not exactly
- *           symmetric is taken as that triangle mirrored)
+ *   A       n x n symmetric FP32 matrix, row-major, leading dimension lda >= n.
+ *           Several kernels read only part of A[S,S] and mirror it (the tuned
+ *           choices for 48 < k <= 192 read A[S[r]][S[c]] for r <= c; the one
+ *           for 192 < k <= 256 reads the upper 32 x 32 tiles), so for an A that
+ *           is not exactly symmetric the result depends on the kernel chosen
+ *           for k.
  *   idx     concatenated 0-based index sets
  *   offsets NULL: uniform k, set s = idx[s*k .. s*k+k-1];
  *           else CSR (nsets+1 entries), set s = idx[offsets[s] .. offsets[s+1])
