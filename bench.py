@@ -400,7 +400,8 @@ def run_ours(args):
             "precision": "FP32 vectors and matvecs; FP64 alpha/beta accumulation and Sturm bisection",
             "config": config_dict(ws),
             "e2e": {"value": NSETS / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "path": "pl_solve_host (C ABI, pinned host buffers)"},
+                    "d2h_bytes_per_step": int(d2h), "path": "pl_solve_host (C ABI, pinned host buffers: A copied in before the launch; the sets read by the "
+                            "kernel from pinned host memory while it computes; results copied out)"},
             "gpu_launches": args.steps,
             "plain": {"value": NSETS / (plain_ms * 1e-3), "unit": "solves/s", "ms_per_step": plain_ms,
                       "form": "one set per thread block (PL_FORM_PLAIN)"},
