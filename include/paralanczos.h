@@ -100,7 +100,13 @@ int pl_solve_noalloc(const float *A, int n, long long lda, const int *idx, long 
                      double *lmin, double *lmax, double *delta, int *err, void *stream);
 
 /* Same with HOST buffers: copies A and the sets in, solves, copies results out
- * (synchronous).  offsets/eig/det/lmin/lmax/delta/err nullable as above.     */
+ * (synchronous).  offsets/eig/det/lmin/lmax/delta/err nullable as above.
+ * With uniform k, extremes only, and a k whose kernel reads each set's indices
+ * one set ahead (the built-in choice for 48 < k <= 64), an idx array in pinned
+ * host memory that is mapped into the device's address space (cudaMallocHost,
+ * cudaHostAlloc, or registered with cudaHostRegister) is not copied: the
+ * kernel reads it over the host link while it computes.  The results are the
+ * same either way.                                                          */
 int pl_solve_host(const float *A, int n, long long lda, const int *idx, const long long *offsets,
                   long long nsets, int k, int form, double *lmin, double *lmax, double *delta,
                   int *err, double *eig, double *det);
