@@ -106,12 +106,15 @@ def run_c1(args):
     ms_plain, _ = _timed_steps(lambda: api.solve(A, idx, k=k, form="plain", out=outp), 3, 2, flush, stream)
     lmin = out["lmin"].cpu().numpy()
     lmax = out["lmax"].cpu().numpy()
-    worst = worst_all = 0.0
+    errs = np.empty(2 * nsets)
+    worst_all = 0.0
     for s in range(nsets):
         S = idx_h[s * k:(s + 1) * k]
         w = B.dsyev_eigs(A64[np.ix_(S, S)])
-        worst = max(worst, abs(lmin[s] - w[0]) / w[0], abs(lmax[s] - w[-1]) / w[-1])
+        errs[2 * s] = abs(lmin[s] - w[0]) / w[0]
+        errs[2 * s + 1] = abs(lmax[s] - w[-1]) / w[-1]
         worst_all = max(worst_all, np.max(np.abs(eig[s * k:(s + 1) * k] - w)) / np.max(np.abs(w)))
+    worst = float(np.max(errs))
     cpu = None
     if not args.no_cpu:
         O.use_reference_tqlrat(True)
@@ -139,6 +142,7 @@ def run_c1(args):
                      "gpu_launches": args.steps,
                      "plain": {"value": nsets / (ms_plain * 1e-3), "ms_per_step": ms_plain},
                      "accuracy": {"sets_checked": nsets, "max_rel_err_vs_dsyev_extremes": worst,
+                                  "p99_rel_err_vs_dsyev_extremes": float(np.percentile(errs, 99)),
                                   "max_err_all_eigenvalues_drop_in": worst_all},
                      "roofline": {"bound": "fp32", "achieved": 4.0 * k ** 3 * nsets / (ms * 1e-3) / 1e12,
                                   "peak": api.fp32_peak(), "unit": "TFLOP/s", "traffic": None,
@@ -183,15 +187,19 @@ def run_c3(args):
     lmin = out["lmin"].cpu().numpy()
     lmax = out["lmax"].cpu().numpy()
     err = out["err"].cpu().numpy()
+    # per k: max and p99 of the relative error of lambda_min and lambda_max
+    # against FP64 dsyev over 200 sets of that k spread over the stream
     per_k = {}
     for kv in KV_C3:
-        sel = np.nonzero(ks == kv)[0][:16]
-        worst = 0.0
+        ids = np.nonzero(ks == kv)[0]
+        sel = ids[np.linspace(0, len(ids) - 1, min(200, len(ids))).astype(np.int64)]
+        errs = []
         for s in sel:
             S = idx_h[off_h[s]:off_h[s + 1]]
             w = B.dsyev_eigs(A64[np.ix_(S, S)])
-            worst = max(worst, abs(lmin[s] - w[0]) / abs(w[0]), abs(lmax[s] - w[-1]) / abs(w[-1]))
-        per_k[str(kv)] = {"sets": int(np.sum(ks == kv)), "checked": int(len(sel)), "max_rel_err": worst}
+            errs += [abs(lmin[s] - w[0]) / abs(w[0]), abs(lmax[s] - w[-1]) / abs(w[-1])]
+        per_k[str(kv)] = {"sets": int(len(ids)), "checked": int(len(sel)), "max_rel_err": float(np.max(errs)),
+                          "p99_rel_err": float(np.percentile(errs, 99))}
     # end to end through the C ABI with pinned host buffers
     A_h = A.cpu().pin_memory()
     idx_p = torch.from_numpy(idx_h).pin_memory()
