@@ -180,7 +180,7 @@ int pl_solve_gram(const void *prep, int m, int n, const int *idx, long long nset
  * GPU in up to `max_waves` (at most 4) device-resident request loops, one
  * CUDA graph each (a conditional WHILE node over: plan, expand, binned solve,
  * finish), requests spread over the loops by k.  Each pass a loop forms a
- * wave of about PL_SERVE_WAVE_MS (default 20) ms of GPU work -- the oldest
+ * wave of about PL_SERVE_WAVE_MS (default 10) ms of GPU work -- the oldest
  * unfinished request takes up to PL_SERVE_OLDEST_SHARE (default 0.9) of it,
  * the requests with the least work left the rest, so large requests are split
  * over waves and small ones go first -- and writes results and completion

@@ -19,7 +19,7 @@
 //     requests in device memory: each pass a loop's planning kernel absorbs new
 //     descriptors from the ring (claiming each with a compare-and-swap), scans
 //     the table with a whole CTA, and forms its next "wave" of about
-//     PL_SERVE_WAVE_MS (default 20) ms of estimated GPU work -- the oldest
+//     PL_SERVE_WAVE_MS (default 10) ms of estimated GPU work -- the oldest
 //     unfinished request gets up to PL_SERVE_OLDEST_SHARE (default 0.9) of it,
 //     then the requests with the least work left fill the rest -- claiming the
 //     sets with atomic adds, so two loops never take the same set and no kernel
@@ -357,7 +357,7 @@ struct Server {
   cudaStream_t up = nullptr;  // index uploads at admission
   cudaEvent_t up_ev = nullptr;
   std::vector<Request*> uploading;  // uploaded by up_ev, not yet published
-  double wave_us = 20000.0, oldest_share = 0.9, idle_ms = 20.0;
+  double wave_us = 10000.0, oldest_share = 0.9, idle_ms = 20.0;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<Request*> pending;  // submitted, not admitted (arrival order)

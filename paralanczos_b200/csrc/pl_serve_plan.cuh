@@ -18,9 +18,9 @@ constexpr int kMaxPieces = 2048;          // request pieces one wave can hold
 // inside a bin and never below the previous bin's figure.  Only used to size
 // waves: a misestimate changes wave lengths, never results.
 __host__ __device__ inline double set_cost_us(int k) {
-  const int kb[9] = {8, 16, 32, 64, 128, 192, 256, 384, 512};
-  const double tb[9] = {0.001, 0.003, 0.014, 0.10, 0.88, 8.3, 25.5, 92.0, 253.0};
-  for (int b = 0; b < 9; ++b) {
+  const int kb[11] = {8, 16, 32, 48, 64, 96, 128, 192, 256, 384, 512};
+  const double tb[11] = {0.001, 0.003, 0.0145, 0.045, 0.089, 0.334, 0.74, 3.2, 6.0, 38.9, 115.0};
+  for (int b = 0; b < 11; ++b) {
     if (k <= kb[b]) {
       const double x = (double)k / kb[b];
       const double c = tb[b] * x * x * x;
@@ -28,7 +28,7 @@ __host__ __device__ inline double set_cost_us(int k) {
       return c > lo ? c : lo;
     }
   }
-  return tb[8];
+  return tb[10];
 }
 
 // One admitted request, published by the host into the ring (mapped pinned

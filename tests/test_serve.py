@@ -171,7 +171,9 @@ def test_large_request_split_over_waves_is_exact(mats, monkeypatch):
 
     from paralanczos_b200.api import Server
     rng = np.random.default_rng(7)
-    monkeypatch.setenv("PL_SERVE_WAVE_MS", "0.5")
+    # ~3.2 us of estimated whole-GPU work per set of k = 200: 6.4 ms for the
+    # request, so 0.2 ms waves cut it into some 30 pieces
+    monkeypatch.setenv("PL_SERVE_WAVE_MS", "0.2")
     S = _sets(rng, 2000, 1024, 200)
     with Server(budget_bytes=1 << 30, host_pool_bytes=64 << 20) as srv:
         mid = srv.add_matrix(mats[0])
