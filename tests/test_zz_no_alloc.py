@@ -53,7 +53,7 @@ def _noalloc(A, idx, k):
 
 def test_noalloc_matches_pl_solve_on_two_calls_in_a_row():
     import torch
-    for call, (k, nsets, seed) in enumerate([(64, 3000, 11), (16, 5000, 12)]):
+    for call, (k, nsets, seed) in enumerate([(64, 3000, 11), (16, 5000, 12), (48, 4000, 13)]):
         A_np = _gram(1024, 2048, seed)
         _, idx_np = O.gen_stream(seed, 0, nsets, 2048, 0, k, k)
         A = torch.from_numpy(A_np).cuda()
