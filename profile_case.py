@@ -9,10 +9,12 @@ profiler can skip the first launch and capture the next ones:
         python profile_case.py --case k64
 
 Cases:
+  k48      batched form, k = 48 (the k <= 48 bin's kernel) on the k64 matrix.
   k64      batched form, k = 64, A = Phi^T Phi (Phi 1024 x 4096 N(0, 1/1024),
            workloads.c2_matrix), sets from the counter-based generator
            (seed 1); the tuned variant.
   plain64  the same sets through the one-set-per-block form.
+  k96      batched form, k = 96 (the k <= 96 bin's kernel) on the same matrix.
   k128     batched form, k = 128 on the same matrix.
   k192     batched form, k = 192 (one-SM engine of the cluster kernel).
   k256     batched form, k = 256 (thread-block-cluster engine).
@@ -34,7 +36,8 @@ sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--case", required=True,
-                    choices=["k64", "plain64", "k128", "k192", "k256", "gram", "uneven", "gather"])
+                    choices=["k48", "k64", "plain64", "k96", "k128", "k192", "k256", "gram", "uneven",
+                             "gather"])
     ap.add_argument("--nsets", type=int, default=0)
     ap.add_argument("--launches", type=int, default=2)
     ap.add_argument("--variant", type=int, default=-2,
@@ -46,7 +49,7 @@ def main(argv=None) -> int:
     import workloads as W
     from paralanczos_b200 import api
     if a.variant >= -1:
-        kb = {"k64": 64, "plain64": 64, "k128": 128, "k192": 192, "k256": 256, "gram": 128, "uneven": 0,
+        kb = {"k48": 48, "k64": 64, "plain64": 64, "k96": 96, "k128": 128, "k192": 192, "k256": 256, "gram": 128, "uneven": 0,
               "gather": 64}[a.case]
         b = next(i for i in range(api.num_bins()) if api.bin_kmax(i) >= kb) if kb else 0
         api.tune_set(b, a.variant)
@@ -80,8 +83,8 @@ def main(argv=None) -> int:
             for _ in range(a.launches):
                 api.solve(A, idx, offsets=off, out=out)
         else:
-            k = {"k64": 64, "plain64": 64, "k128": 128, "k192": 192, "k256": 256}[a.case]
-            nsets = a.nsets or {64: 200_000, 128: 40_000, 192: 8_000, 256: 4_000}[k]
+            k = {"k48": 48, "k64": 64, "plain64": 64, "k96": 96, "k128": 128, "k192": 192, "k256": 256}[a.case]
+            nsets = a.nsets or {48: 300_000, 64: 200_000, 96: 80_000, 128: 40_000, 192: 8_000, 256: 4_000}[k]
             form = "plain" if a.case == "plain64" else "batched"
             idx = api.gen_sets(1, 0, nsets, n, k)
             out = api.solve(A, idx, k=k, form=form)
