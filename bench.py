@@ -161,19 +161,6 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-def tuned_variant(b: int) -> int:
-    """Variant of bin b the autotuner chose for this GPU (0 = compiled default)."""
-    p = os.path.join(ROOT, "paralanczos_b200", "tuning.json")
-    try:
-        import torch
-        data = json.load(open(p))
-        if data.get("device") == torch.cuda.get_device_name():
-            return int(data["bins"][str(b)]["variant"])
-    except Exception:
-        pass
-    return 0
-
-
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -393,6 +380,7 @@ def run_ours(args):
                "lapack_dsyevr": {"value": lr, "sets": ln, "note": "extremes only, one set per call, FP64"}}
 
     if rank == 0:
+        bin_k = next(b for b in range(api.num_bins()) if api.bin_kmax(b) >= K)  # the bin k = 64 runs in
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -400,8 +388,9 @@ def run_ours(args):
             "precision": "FP32 vectors and matvecs; FP64 alpha/beta accumulation and Sturm bisection",
             "config": config_dict(ws),
             "e2e": {"value": NSETS / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "path": "pl_solve_host (C ABI, pinned host buffers: A copied in before the launch; the sets read by the "
-                            "kernel from pinned host memory while it computes; results copied out)"},
+                    "d2h_bytes_per_step": int(d2h),
+                    "path": "pl_solve_host (C ABI, pinned host buffers: A copied in before the launch; the sets "
+                            "read by the kernel from pinned host memory while it computes; results copied out)"},
             "gpu_launches": args.steps,
             "plain": {"value": NSETS / (plain_ms * 1e-3), "unit": "solves/s", "ms_per_step": plain_ms,
                       "form": "one set per thread block (PL_FORM_PLAIN)"},
@@ -409,7 +398,7 @@ def run_ours(args):
             "accuracy": acc,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
                          "frac": achieved / peak_fp32, "traffic": traffic,
-                         "kernel": api.tune_describe(3, tuned_variant(3))[1],
+                         "kernel": api.tune_describe(bin_k, api.tune_get(bin_k))[1],
                          "peak_source": "FP32 FMA peak measured live by k_fma_peak (no FP32 figure in "
                                         "MEASURED_PEAKS.json)",
                          "algorithmic": "4k^3 FLOP per set (k matvecs + one reorthogonalisation pass)"},

@@ -244,6 +244,9 @@ int pl_launch_reference_kernel(const char *name, unsigned grid_x, unsigned block
  * pl_tune_describe); -1 restores the built-in default (the autotuner's
  * choice on B200).                                                          */
 int pl_tune_set(int bin, int variant);
+/* The variant bin `bin` runs now (as selected by pl_tune_set or the built-in
+ * default); -1 for an unknown bin.  No counterpart in the reference.        */
+int pl_tune_get(int bin);
 /* Writes a description of bin/variant into buf (NUL-terminated); returns the
  * number of variants of `bin`, or 0 for an unknown bin.                      */
 int pl_tune_describe(int bin, int variant, char *buf, int buflen);

@@ -19,6 +19,7 @@ from .api import (  # noqa: F401
     solve,
     solve_host,
     tune_describe,
+    tune_get,
     tune_set,
 )
 from ._lib import PLError, lib  # noqa: F401

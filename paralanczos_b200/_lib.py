@@ -39,6 +39,7 @@ SIGNATURES = {
     "pl_calculate_subeigs2": (_i, [_vp, _i, _i, _vp, _vp, _vp, _i]),
     "pl_calculate_eigs": (_i, [_vp, _i, _vp, _vp]),
     "pl_tune_set": (_i, [_i, _i]),
+    "pl_tune_get": (_i, [_i]),
     "pl_tune_describe": (_i, [_i, _i, C.c_char_p, _i]),
     "pl_num_bins": (_i, []),
     "pl_bin_kmax": (_i, [_i]),

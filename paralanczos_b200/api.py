@@ -231,6 +231,11 @@ def tune_describe(b: int, variant: int = 0) -> tuple[int, str]:
     return n, buf.value.decode()
 
 
+def tune_get(b: int) -> int:
+    """The variant bin b runs now (-1 for an unknown bin)."""
+    return lib().pl_tune_get(b)
+
+
 def tune_set(b: int, variant: int) -> None:
     check(lib().pl_tune_set(b, variant), "pl_tune_set")
 

@@ -166,11 +166,12 @@ size_t scratch_sar() {
   return grid * (CTA / NT) * (NT / 2) * KB * sizeof(double2);
 }
 
-// shared-A with the next set's triangle prefetched (extremes mode)
-template <int KB, int RPT, int CTA, int REGS>
+// shared-A with the next set's triangle prefetched (extremes mode); AR float4
+// chunks of each row of A_S in registers
+template <int KB, int RPT, int CTA, int REGS, int AR = 0>
 cudaError_t launch_sap(const MatrixF32& M, const SetSource& src, const SetOutputs& out, long long nitems,
                        void* scratch, cudaStream_t st, bool prep) {
-  auto kern = k_sa_solve_p<KB, RPT, CTA, REGS>;
+  auto kern = k_sa_solve_p<KB, RPT, CTA, REGS, AR>;
   constexpr int GPC = CTA / CfgSA<KB, RPT>::NT;
   const size_t dsm = (sizeof(SASmem<KB, RPT>) + sizeof(SAStage<KB, CfgSA<KB, RPT>::NT>)) * GPC;
   static int occ = [&] {
@@ -187,9 +188,9 @@ cudaError_t launch_sap(const MatrixF32& M, const SetSource& src, const SetOutput
   return cudaGetLastError();
 }
 
-template <int KB, int RPT, int CTA, int REGS>
+template <int KB, int RPT, int CTA, int REGS, int AR = 0>
 size_t scratch_sap() {
-  auto kern = k_sa_solve_p<KB, RPT, CTA, REGS>;
+  auto kern = k_sa_solve_p<KB, RPT, CTA, REGS, AR>;
   constexpr int NT = CfgSA<KB, RPT>::NT;
   const size_t dsm = (sizeof(SASmem<KB, RPT>) + sizeof(SAStage<KB, CfgSA<KB, RPT>::NT>)) * (CTA / NT);
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
@@ -359,6 +360,12 @@ struct Variant {
         {launch_sap<KB, RPT, CTA, REGS>, nullptr}, {scratch_sap<KB, RPT, CTA, REGS>, scratch_none}, \
         true                                                                                     \
   }
+#define SAPR(KB, RPT, CTA, REGS, AR)                                                         \
+  Variant {                                                                                    \
+    "sharedA prefetch KB=" #KB " RPT=" #RPT " CTA=" #CTA " REGS=" #REGS " AREG=" #AR,          \
+        {launch_sap<KB, RPT, CTA, REGS, AR>, nullptr},                                          \
+        {scratch_sap<KB, RPT, CTA, REGS, AR>, scratch_none}, true                               \
+  }
 #define SA2(KB, CTA, MINB)                                                                   \
   Variant {                                                                                    \
     "sharedA 2 threads/row KB=" #KB " CTA=" #CTA " MINB=" #MINB,                               \
@@ -398,7 +405,7 @@ const std::vector<Variant>& variants(int b) {
       {SA(48, 3, 128, 2), REG(48, 3, 2, 128, 2)},
       {REG(64, 1, 1, 128, 3), SA(64, 2, 128, 3), REG(64, 1, 1, 128, 2), SA(64, 2, 128, 2),
        SAR(64, 2, 96, 224), SAR(64, 2, 128, 224), SAR(64, 2, 64, 200), SAP(64, 2, 128, 224),
-       SAP(64, 2, 64, 224), SAP(64, 2, 96, 224)},
+       SAP(64, 2, 64, 224), SAP(64, 2, 96, 224), SAPR(64, 2, 128, 255, 4), SAPR(64, 2, 64, 255, 4)},
       {SA(96, 1, 96, 3), SA2(96, 96, 3), SA2(96, 96, 4), SA(96, 1, 96, 4)},
       {SA(128, 1, 128, 3), REG(128, 1, 2, 256, 1), SA(128, 1, 128, 2), SA2(128, 128, 2), SYM(4, 5, 2, 3),
        SYM(4, 10, 1, 2)},
@@ -417,8 +424,8 @@ const std::vector<Variant>& variants(int b) {
 
 // Built-in shape per bin: the autotuner's choices on B200 (tuning.json), so a
 // caller that never runs the Python tuner (a C program, MATLAB) gets them too.
-const int kDefaultVariant[kNumBins] = {0, 0, 2, 0, 7, 1, 3, 6, 7, 6, 3};
-int g_variant[kNumBins] = {0, 0, 2, 0, 7, 1, 3, 6, 7, 6, 3};
+const int kDefaultVariant[kNumBins] = {0, 0, 2, 1, 10, 1, 3, 6, 7, 6, 3};
+int g_variant[kNumBins] = {0, 0, 2, 1, 10, 1, 3, 6, 7, 6, 3};
 
 int bin_of_k(int k) {
   for (int b = 0; b < kNumBins; ++b)
@@ -1084,6 +1091,12 @@ int pl_tune_set(int bin, int variant) {
   if (variant >= (int)variants(bin).size()) return PL_EINVAL;
   g_variant[bin] = variant < 0 ? kDefaultVariant[bin] : variant;
   return PL_OK;
+}
+
+int pl_tune_get(int bin) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (bin < 0 || bin >= kNumBins) return -1;
+  return g_variant[bin];
 }
 
 int pl_tune_describe(int bin, int variant, char* buf, int buflen) {

@@ -130,7 +130,7 @@ struct TriPrefetch {
   }
 };
 
-template <int KB, int RPT, bool ALL, bool PF = false>
+template <int KB, int RPT, bool ALL, bool PF = false, int AR = 0>
 __device__ __forceinline__ int solve_set_sa(const MatrixF32& M, const int* __restrict__ S, int k,
                                              long long set, long long off, const SetOutputs& out,
                                              SASmem<KB, RPT>& sm,
@@ -283,6 +283,15 @@ __device__ __forceinline__ int solve_set_sa(const MatrixF32& M, const int* __res
   float sc = 1.f, bprev = 0.f;
   int status = 0;
   g.sync();
+  // The first AR float4 chunks of each of the thread's rows of A_S are held in
+  // registers for the whole recurrence: AR * RPT fewer shared-memory loads per
+  // step (the L1 data pipe is the kernel's busiest unit), same products.
+  static_assert(AR >= 0 && AR <= NCH, "register chunks of a row");
+  float4 Ar[RPT][AR > 0 ? AR : 1];
+#pragma unroll
+  for (int q = 0; q < RPT; ++q)
+#pragma unroll
+    for (int ch = 0; ch < AR; ++ch) Ar[q][ch] = my[(q * NCH + ch) * NT];
 
   for (int j = 0; j < k; ++j) {
     if constexpr (PF) pre.step(stg, t);
@@ -301,7 +310,7 @@ __device__ __forceinline__ int solve_set_sa(const MatrixF32& M, const int* __res
       const float2 b01 = make_float2(b4.x, b4.y), b23 = make_float2(b4.z, b4.w);
 #pragma unroll
       for (int q = 0; q < RPT; ++q) {
-        const float4 a4 = my[(q * NCH + ch) * NT];
+        const float4 a4 = ch < AR ? Ar[q][ch < AR ? ch : 0] : my[(q * NCH + ch) * NT];
         Pr[q][2 * ch] = __ffma2_rn(ncoef[q], b01, Pr[q][2 * ch]);
         Pr[q][2 * ch + 1] = __ffma2_rn(ncoef[q], b23, Pr[q][2 * ch + 1]);
         ya[q] = __ffma2_rn(make_float2(a4.x, a4.y), b01, ya[q]);

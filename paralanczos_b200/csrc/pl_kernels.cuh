@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(CTA, MINB)
 // Batched form, shared-A engine (pl_engine_sa.cuh): persistent, A_S in
 // dynamic shared memory, P in registers.
 // ---------------------------------------------------------------------------
-template <int KB, int RPT, int CTA, bool ALL, bool PF = false>
+template <int KB, int RPT, int CTA, bool ALL, bool PF = false, int AR = 0>
 __device__ __forceinline__ void sa_solve_body(const MatrixF32& M, const SetSource& src, const SetOutputs& out,
                                               double2* __restrict__ qbuf) {
   using C = CfgSA<KB, RPT>;
@@ -120,7 +120,7 @@ __device__ __forceinline__ void sa_solve_body(const MatrixF32& M, const SetSourc
       if (g.t == 0) qmeta[gic][nq] = QueueMeta{set, k, 0};
     }
     bool issued = false;
-    const int st = solve_set_sa<KB, RPT, ALL, PF>(M, src.idx + off, k, set, off, out, smem[gic], g, stg, have,
+    const int st = solve_set_sa<KB, RPT, ALL, PF, AR>(M, src.idx + off, k, set, off, out, smem[gic], g, stg, have,
                                                   &nx, &issued);
     have = issued;
     if constexpr (!ALL) {
@@ -159,11 +159,11 @@ __global__ void __maxnreg__(REGS) k_sa_solve_r(MatrixF32 M, SetSource src, SetOu
 }
 
 // The same with the next set's triangle prefetched into a shared-memory stage
-// (extremes mode).
-template <int KB, int RPT, int CTA, int REGS>
+// (extremes mode); AR float4 chunks of each row of A_S also held in registers.
+template <int KB, int RPT, int CTA, int REGS, int AR = 0>
 __global__ void __maxnreg__(REGS) k_sa_solve_p(MatrixF32 M, SetSource src, SetOutputs out,
                                                double2* __restrict__ qbuf) {
-  sa_solve_body<KB, RPT, CTA, false, true>(M, src, out, qbuf);
+  sa_solve_body<KB, RPT, CTA, false, true, AR>(M, src, out, qbuf);
 }
 
 // ---------------------------------------------------------------------------

@@ -5,7 +5,9 @@ the ones the direct gather loads, so every result must be bitwise equal to the
 same shape without the prefetch; checked on a uniform stream, on an uneven
 (CSR) stream whose sets change k from one set to the next, with sets carrying
 an index outside [0, n) and a set whose k is out of range in between (their
-neighbours are prefetched around them), and against FP64 dsyev.
+neighbours are prefetched around them), and against FP64 dsyev.  The variants
+that also hold some float4 chunks of each row of A_S in registers (AREG) are
+compared bitwise with the prefetch shape of the same CTA without them.
 """
 import numpy as np
 import pytest
@@ -29,9 +31,17 @@ def _pairs():
         for b in range(api.num_bins()):
             if api.bin_kmax(b) not in (32, 64):
                 continue
+            descs = [api.tune_describe(b, w)[1] for w in range(api.tune_describe(b, 0)[0])]
             for v in _variants(b, "prefetch"):
-                d = api.tune_describe(b, v)[1].replace("sharedA prefetch ", "sharedA ")
-                base = [w for w in range(api.tune_describe(b, 0)[0]) if api.tune_describe(b, w)[1] == d]
+                d = descs[v]
+                if " AREG=" in d:
+                    # chunks of A_S in registers: the same prefetch shape (KB,
+                    # RPT, CTA) without them is the reference
+                    stem = d.split(" REGS=")[0] + " REGS="
+                    base = [w for w, e in enumerate(descs) if e.startswith(stem) and " AREG=" not in e]
+                else:
+                    d = d.replace("sharedA prefetch ", "sharedA ")
+                    base = [w for w, e in enumerate(descs) if e == d]
                 out.append((b, v, base[0] if base else -1))
         return out
     except Exception:
