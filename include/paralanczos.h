@@ -160,7 +160,11 @@ long long pl_gram_prep_bytes(int m, int n);
 int pl_gram_prepare(const float *Phi, long long ld, int m, int n, void *prep, void *stream);
 /* The Gram blocks themselves: blocks[s*k*k + i*k + j] = (Phi_S^T Phi_S)_ij
  * (device FP32), err[s] = PL_SET_BAD_INDEX for a set with an index outside
- * [0, n).  Synchronous (returns PL_ETIMEDOUT if a bounded wait gave up).     */
+ * [0, n).  Each block is formed from the bf16 split and then scaled as
+ * d_i d_j B_ij with d_i = sqrt(||column S_i of Phi||^2 / B_ii) (the exact
+ * squared norms are part of the prepared frame), so its diagonal is exact
+ * and it stays exactly symmetric.  Synchronous (returns PL_ETIMEDOUT if a
+ * bounded wait gave up).                                                    */
 int pl_gram_blocks(const void *prep, int m, int n, const int *idx, long long nsets, int k,
                    float *blocks, int *err, void *stream);
 /* Form and solve: outputs as pl_solve (device pointers; eig at s*k).  Works

@@ -16,7 +16,16 @@
 // i.e. three bf16 products per K step (the budget of the usual bf16x3 split),
 // with the cross terms folded by symmetry so that the lo lo^T term fits in the
 // same budget; the result is exactly symmetric.  The only lost bits are the
-// residual x - hi - lo (below 2^-16 |x|).
+// residual x - hi - lo (below 2^-16 |x|).  Its systematic part, and that of
+// the FP32 accumulation of the diagonal (a sum of same-sign terms), is
+// compensated per set: the preparation also stores each column's exact
+// squared norm ||Phi_c||^2 (an FP64 sum, stored FP32), and the block is
+// written as d_i d_j A_S[i][j] with d_i = sqrt(||Phi_S_i||^2 / A_S[i][i]), so
+// its diagonal is the exact squared norm (a congruence: symmetry and
+// definiteness are kept).  A frame whose entries share one magnitude (a
+// Rademacher frame, represented by the split as one multiple of itself) is
+// then reproduced to a few FP32 roundings; for other frames the random part
+// of the residual remains.
 //
 // Kernel structure (one persistent CTA per SM, 288 threads):
 //   warps 0-3  gather: cp.async of the set's 128 column records per 64-row
@@ -178,15 +187,29 @@ __global__ void __launch_bounds__(256) k_gram_split(const float* __restrict__ Ph
   }
 }
 
+// Exact squared column norms for the compensation: nrm2[c] = ||Phi_c||^2
+// over all m rows (FP64 sum, stored FP32).
+__global__ void __launch_bounds__(256) k_gram_colnorm(const float* __restrict__ Phi, long long ld, int m,
+                                                      int n, float* __restrict__ nrm2) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    double ex = 0.0;
+    for (int r = 0; r < m; ++r) {
+      const double x = (double)Phi[(size_t)r * ld + c];
+      ex = fma(x, x, ex);
+    }
+    nrm2[c] = (float)ex;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Batched Gram blocks of sets [0, nsets) (uniform k <= 128): block s at
 // blocks + s * k * k, row-major, exactly symmetric.  gerr[s] |= SET_BAD_INDEX
 // for a set with an index outside [0, n) (its rows read as zero).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(NTHREADS, 1)
-    k_gram(const char* __restrict__ prep, int n, int kc_total, const int* __restrict__ idx,
-           long long nsets, int k, float* __restrict__ blocks, int* __restrict__ gerr,
-           int* __restrict__ status, int hold) {
+    k_gram(const char* __restrict__ prep, const float* __restrict__ nrm2, int n, int kc_total,
+           const int* __restrict__ idx, long long nsets, int k, float* __restrict__ blocks,
+           int* __restrict__ gerr, int* __restrict__ status, int hold) {
   extern __shared__ unsigned char smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
@@ -392,12 +415,27 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       }
       tc_fence_before();
       mbar_arrive(d2empty_bar(a));
+      // this row's compensation d = sqrt(exact squared norm / formed
+      // diagonal), kept in the row's padding slot of E (column ROWS, never an
+      // accumulator); 1 for an invalid index or a non-positive norm
+      float dr = 1.f;
+      if (row < k) {
+        const int gi = __ldg(idx + set * (long long)k + row);
+        const float dg = Er[row];
+        if (gi >= 0 && gi < n) {
+          const float ex = __ldg(nrm2 + gi);
+          if (ex > 0.f && dg > 0.f) dr = (float)sqrt((double)ex / (double)dg);
+        }
+      }
+      Er[ROWS] = dr;
       asm volatile("bar.sync 1, %0;" ::"n"(NEPI) : "memory");
       if (row < k) {
         float* dst = blocks + (size_t)set * k * k + row;
+        // (both operand pairs commute, so element (c, row) written by thread
+        // c is bitwise element (row, c): the block stays exactly symmetric)
 #pragma unroll 4
         for (int c = 0; c < k; ++c)
-          dst[(size_t)c * k] = 0.5f * (Er[c] + E[c * EPAD + row]);
+          dst[(size_t)c * k] = (0.5f * (Er[c] + E[c * EPAD + row])) * (dr * E[c * EPAD + ROWS]);
       }
       asm volatile("bar.sync 1, %0;" ::"n"(NEPI) : "memory");
     }
@@ -496,8 +534,9 @@ int launch_gram(const void* prep, int m, int n, const int* idx, long long nsets,
   // the kernel frees its TMEM and returns, and the call reports PL_ETIMEDOUT.
   const char* h = getenv("PL_GRAM_TEST_HOLD");
   const int hold = (h && h[0] == '1') ? 1 : 0;
-  k_gram<<<(unsigned)grid, NTHREADS, kSmemBytes, st>>>((const char*)prep, n, kc_total, idx, nsets, k,
-                                                       blocks, gerr, status, hold);
+  const float* nrm2 = (const float*)((const char*)prep + (size_t)n * kc_total * REC_BYTES);
+  k_gram<<<(unsigned)grid, NTHREADS, kSmemBytes, st>>>((const char*)prep, nrm2, n, kc_total, idx, nsets,
+                                                       k, blocks, gerr, status, hold);
   GCU(cudaGetLastError());
   return PL_OK;
 }
@@ -549,7 +588,8 @@ extern "C" {
 long long pl_gram_prep_bytes(int m, int n) {
   if (m < 1 || n < 1) return -1;
   const long long kc = (m + KCH - 1) / KCH;
-  return (long long)n * kc * REC_BYTES;
+  // the column records, then each column's exact squared norm (FP32)
+  return (long long)n * kc * REC_BYTES + (((long long)n * 4 + 255) & ~255LL);
 }
 
 int pl_gram_prepare(const float* Phi, long long ld, int m, int n, void* prep, void* stream) {
@@ -557,6 +597,10 @@ int pl_gram_prepare(const float* Phi, long long ld, int m, int n, void* prep, vo
   const int kc_total = (m + KCH - 1) / KCH;
   dim3 grid((unsigned)((n + KCH - 1) / KCH), (unsigned)kc_total);
   k_gram_split<<<grid, 256, 0, (cudaStream_t)stream>>>(Phi, ld, m, n, kc_total, (__nv_bfloat16*)prep);
+  GCU(cudaGetLastError());
+  float* nrm2 = (float*)((char*)prep + (size_t)n * kc_total * REC_BYTES);
+  const int gb = (n + 255) / 256;
+  k_gram_colnorm<<<(unsigned)(gb < 4096 ? gb : 4096), 256, 0, (cudaStream_t)stream>>>(Phi, ld, m, n, nrm2);
   GCU(cudaGetLastError());
   return PL_OK;
 }

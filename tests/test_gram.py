@@ -4,9 +4,10 @@ Spec: the reference's subset Gram kernel DSG_B (ParaLanczos.cu:364-382),
 restated in the oracle as ``dsg_b`` (FP64).  The GPU forms the block from a
 bf16 split of the FP32 frame (x = hi + lo, lo2 = 2 lo rounded to bf16) as
 F = hi hi^T + hi lo2^T + lo2 lo2^T / 4 with FP32 accumulation and returns
-(F + F^T) / 2.  Checked three ways: against that arithmetic evaluated in FP64
-(only the FP32 accumulation differs), against the oracle's FP64 DSG_B
-(the split's truncation, below 2^-16 relative per entry), and the eigenvalues
+d_i d_j (F + F^T)_ij / 2, where d_c = ||Phi_c|| / ||hi_c + lo_c|| compensates
+the split's residual per column.  Checked three ways: against that arithmetic
+evaluated in FP64 (only the FP32 accumulation differs), against the oracle's
+FP64 DSG_B (the split's truncation, below 2^-16 relative per entry), and the eigenvalues
 of the solve against LAPACK dsyev on the FP64 Gram of the FP32 frame
 (<= 1e-5 relative).
 """
@@ -35,14 +36,20 @@ def _sets(nsets, n, k, seed):
 
 
 def _split_model(Phi, S):
-    """The kernel's arithmetic in FP64: bf16 pieces, exact products."""
+    """The kernel's arithmetic in FP64: bf16 pieces, exact products, and the
+    per-column compensation d (rounded to FP32, as the kernel stores it)."""
     import torch
     X = torch.from_numpy(np.ascontiguousarray(Phi[:, S].T))          # k x m FP32
     hi = X.to(torch.bfloat16).float()
     lo2 = (2.0 * (X - hi)).to(torch.bfloat16).float()
     H, L = hi.double().numpy(), lo2.double().numpy()
     F = H @ H.T + H @ L.T + (L @ L.T) / 4.0
-    return (F + F.T) / 2.0
+    Xr = H + L / 2.0
+    ex = np.sum(X.double().numpy() ** 2, axis=1)
+    rp = np.sum(Xr ** 2, axis=1)
+    d = np.where((rp > 0) & (ex > 0), np.sqrt(ex / np.where(rp > 0, rp, 1.0)), 1.0).astype(np.float32)
+    d = d.astype(np.float64)
+    return (F + F.T) / 2.0 * np.outer(d, d)
 
 
 def _gpu_frame(Phi):
@@ -75,6 +82,27 @@ def test_gram_blocks_match_split_model_and_dsg_b(m, n, k):
         assert np.max(np.abs(blocks[s] - model) / scale) < 2e-6, s
         ref = O.dsg_b(Phi64, S[s])
         assert np.max(np.abs(blocks[s] - ref) / scale) < 1e-5, s
+
+
+def test_gram_rademacher_frame_compensated_to_fp32_accumulation():
+    """A frame whose entries share one magnitude (+-1/sqrt(m)) is represented
+    by the split as the same multiple of itself everywhere; the per-column
+    compensation removes that factor, so the blocks agree with the FP64 DSG_B
+    to the FP32 accumulation (without it they are off by ~4e-6 relative)."""
+    import torch
+
+    from oracle import oracle as O
+    m, n, k = 2048, 4096, 128
+    Phi = _frame(m, n, "rademacher", 13)
+    S = _sets(24, n, k, 14)
+    blocks, err = _gpu_frame(Phi).blocks(torch.from_numpy(S.reshape(-1)).cuda(), k)
+    blocks = blocks.cpu().numpy().astype(np.float64)
+    assert (err.cpu().numpy() == 0).all()
+    Phi64 = Phi.astype(np.float64)
+    for s in range(len(S)):
+        ref = O.dsg_b(Phi64, S[s])
+        scale = np.sqrt(np.outer(np.diag(ref), np.diag(ref)))
+        assert np.max(np.abs(blocks[s] - ref) / scale) < 1e-6, s
 
 
 def test_gram_many_sets_every_cta_wraps_the_ring():
